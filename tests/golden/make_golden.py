@@ -1,0 +1,54 @@
+"""Generate the golden fixtures that pin the oracle (run on a machine with a GPU).
+
+For every variant and every trace of traces.py, the reference allocator itself
+(oracle/_ref/libouro_ref.so, the reference's headers compiled for sm_100a by
+oracle/Makefile) replays the trace with one GPU thread on a fresh 1 GiB heap.
+The byte offsets it returns (page address minus the reference's d_data) and its
+counters after the trace are written to trace_<variant>.npz.  The reference has
+no tests or known-answer vectors of its own; these fixtures are its outputs.
+
+    python tests/golden/make_golden.py <out_dir>
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from tests.golden import traces  # noqa: E402
+
+
+def ops_digest(ops: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(ops, dtype=np.uint32).tobytes()).hexdigest()
+
+
+def main(out_dir: str) -> int:
+    os.makedirs(out_dir, exist_ok=True)
+    built = {name: traces.build(name) for name in traces.TRACES}
+    for v in oracle.VARIANTS:
+        arrays = {}
+        for name, (ops, tid, bid) in built.items():
+            ref = oracle.RefDriver(v, traces.HEAP_BYTES)
+            if "init_state" not in arrays:
+                arrays["init_state"] = ref.state()
+                info = ref.info()
+                arrays["meta"] = np.array([info["max_chunks"], info["allocation_bytes"]], dtype=np.uint64)
+            off = ref.run_trace(ops, tid, bid)
+            arrays[f"{name}_off"] = off
+            arrays[f"{name}_state"] = ref.state()
+            arrays[f"{name}_ops_sha256"] = np.frombuffer(bytes.fromhex(ops_digest(ops)), dtype=np.uint8)
+            ref.close()
+            print(f"{v:4s} {name:12s} ops={ops.size // 2} next_free_chunk={arrays[f'{name}_state'][0]}", flush=True)
+        np.savez_compressed(os.path.join(out_dir, f"trace_{v}.npz"), **arrays)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else HERE))

@@ -1,0 +1,129 @@
+"""Deterministic request traces for the sequential parity checks.
+
+A trace is a flat uint32 array of (kind, arg) pairs: kind 0 = malloc(arg bytes),
+kind 1 = free(the pointer returned by op number arg).  The same traces are
+replayed by one GPU thread through the reference build (make_golden.py), by the
+C oracle and by the CUDA allocator of this repository.  Every trace stays far
+from the heap's capacity and from the reference's queue limits, so that the
+reference runs it with defined behaviour.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+HEAP_BYTES = 1 << 30
+
+
+class _Builder:
+    def __init__(self):
+        self.ops: list[int] = []
+        self.live: list[int] = []
+
+    def malloc(self, size: int) -> int:
+        i = len(self.ops) // 2
+        self.ops += [0, int(size)]
+        self.live.append(i)
+        return i
+
+    def free(self, i: int):
+        self.ops += [1, int(i)]
+        self.live.remove(i)
+
+    def free_all(self, order=None):
+        for i in list(self.live if order is None else order):
+            self.free(i)
+
+    def array(self) -> np.ndarray:
+        return np.asarray(self.ops, dtype=np.uint32)
+
+
+def basic() -> np.ndarray:
+    """Fixed 64 B requests: fill, free every other one, refill, free all."""
+    b = _Builder()
+    first = [b.malloc(64) for _ in range(300)]
+    for i in first[::2]:
+        b.free(i)
+    for _ in range(200):
+        b.malloc(64)
+    b.free_all()
+    return b.array()
+
+
+def mixed(seed: int = 1, n_ops: int = 3000) -> np.ndarray:
+    """Random mix: log-uniform sizes up to 8 KiB, some 8-32 KiB (second
+    instance), a few above 32 KiB (CUDA device heap), one size 0; frees of
+    random live allocations; everything freed at the end."""
+    rng = np.random.default_rng(seed)
+    b = _Builder()
+    b.malloc(0)
+    tier2 = 0
+    for _ in range(n_ops):
+        if b.live and rng.random() < 0.4:
+            b.free(b.live[int(rng.integers(len(b.live)))])
+            continue
+        u = rng.random()
+        if u < 0.90 or tier2 >= 300:
+            size = int(np.exp(rng.uniform(0.0, np.log(8192.0))))
+        elif u < 0.99:
+            size = int(rng.integers(8193, 32769))
+            tier2 += 1
+        else:
+            size = int(rng.integers(32769, 65537))
+        b.malloc(max(size, 1))
+    order = list(b.live)
+    rng.shuffle(order)
+    b.free_all(order)
+    return b.array()
+
+
+def churn(size: int = 16, n: int = 5000, rounds: int = 6) -> np.ndarray:
+    """Many same-class requests: enough queue traffic to allocate, drain and
+    recycle queue chunks of the virtualized variants (2048 entries each)."""
+    b = _Builder()
+    for r in range(rounds):
+        ids = [b.malloc(size) for _ in range(n)]
+        b.free_all(ids if r % 2 == 0 else ids[::-1])
+    return b.array()
+
+
+def chunk_fifo() -> np.ndarray:
+    """Chunk-queue order: fill three 1 KiB chunks (8 pages each), free pages in
+    C, A, B order so they re-enter the queue in that order, then reallocate."""
+    b = _Builder()
+    ids = [b.malloc(1024) for _ in range(24)]
+    a, bb, c = ids[0:8], ids[8:16], ids[16:24]
+    for i in (c[3], a[5], bb[0], a[7], c[6]):
+        b.free(i)
+    for _ in range(7):
+        b.malloc(1000)
+    b.free_all()
+    return b.array()
+
+
+def tier2() -> np.ndarray:
+    """Second instance only: 16 KiB and 32 KiB pages in 4-base-chunk chunks."""
+    b = _Builder()
+    ids = [b.malloc(16384 if i % 3 else 32768) for i in range(60)]
+    for i in ids[::2]:
+        b.free(i)
+    for i in range(40):
+        b.malloc(12000 if i % 2 else 30000)
+    b.free_all()
+    return b.array()
+
+
+# name -> (builder, tid, bid): the GPU thread that replays the trace
+TRACES = {
+    "basic": (basic, 0, 0),
+    "mixed": (lambda: mixed(1), 0, 0),
+    "mixed_t37b5": (lambda: mixed(2), 37, 5),
+    "churn16": (lambda: churn(16), 0, 0),
+    "churn512": (lambda: churn(512, 2500, 4), 0, 0),
+    "chunk_fifo": (chunk_fifo, 0, 0),
+    "tier2": (tier2, 0, 0),
+}
+
+
+def build(name: str):
+    fn, tid, bid = TRACES[name]
+    return fn(), tid, bid
