@@ -1,0 +1,151 @@
+/*
+ * ouroboros_b200.h -- C ABI of the B200 Ouroboros allocator.
+ *
+ * The device-side interface (what kernels call) is the header-only template
+ * ouro::Ouroboros<V> in ouroboros_b200/csrc/ouro/ouroboros.cuh, reached from
+ * C++/CUDA through include/ouroboros_b200.cuh.  This header is the host side:
+ * plain pointers, sizes and status codes, no CUDA or torch types.  Device
+ * buffers are passed as pointers to device memory; `stream` is a cudaStream_t
+ * passed as void* (NULL = the legacy default stream).
+ *
+ * Each entry point names the reference interface it replaces (paths in the
+ * reference project GPUPeople/Ouroboros).
+ */
+#ifndef OUROBOROS_B200_H
+#define OUROBOROS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The six instantiations of include/InstanceDefinitions.cuh:16-34 (the Multi*
+ * types: 16 B .. 8 KiB pages in 8 KiB chunks plus 16/32 KiB pages in 32 KiB
+ * chunks; larger requests go to the CUDA device heap). */
+typedef enum {
+  OURO_P = 0,   /* MultiOuroPQ   page-based, standard array queues            */
+  OURO_C = 1,   /* MultiOuroCQ   chunk-based, standard array queues           */
+  OURO_VAP = 2, /* MultiOuroVAPQ page-based, virtualized array queues         */
+  OURO_VAC = 3, /* MultiOuroVACQ chunk-based, virtualized array queues        */
+  OURO_VLP = 4, /* MultiOuroVLPQ page-based, virtualized linked-list queues   */
+  OURO_VLC = 5  /* MultiOuroVLCQ chunk-based, virtualized linked-list queues  */
+} ouro_variant;
+
+/* Host-side status codes.  The reference exits the process on a CUDA error
+ * (include/Utility.h:10-36, HANDLE_ERROR); these return instead. */
+typedef enum {
+  OURO_OK = 0,
+  OURO_ERR_ARG = 1,      /* bad argument                                  */
+  OURO_ERR_CUDA = 2,     /* a CUDA runtime call failed                    */
+  OURO_ERR_NOMEM = 3,    /* cudaMalloc of the heap failed                 */
+  OURO_ERR_DEVICE = 4    /* the device reported an allocator error flag   */
+} ouro_status;
+
+/* Device-side error flags (ouro_heap_status.flags). */
+#define OURO_FLAG_OOM 1u        /* some malloc returned nullptr (heap exhausted)    */
+#define OURO_FLAG_TIMEOUT 2u    /* a bounded wait gave up; the heap needs a reset   */
+#define OURO_FLAG_CORRUPT 4u    /* a structural check failed                        */
+#define OURO_FLAG_QUEUE_FULL 8u /* a size class reached its queue capacity          */
+
+typedef struct ouro_heap ouro_heap;
+
+/* Ouroboros<...>::initialize(instantiation_size)  (include/device/Ouroboros.cuh:281,
+ * include/device/MemoryInitialization.cuh:123-219).  Allocates and initializes a
+ * heap of `heap_bytes` on the current device; the number of usable 8 KiB chunks
+ * is the reference's for the same size.  Synchronous. */
+int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out);
+
+/* Memory::~Memory  (include/device/Ouroboros.cuh:11-15): frees the heap. */
+int ouro_destroy(ouro_heap* h);
+
+/* Ouroboros<...>::getDeviceMemoryManager()  (include/device/Ouroboros.cuh:297):
+ * the device pointer kernels call malloc/free on (an ouro::Ouroboros<V>*). */
+void* ouro_device_handle(const ouro_heap* h);
+
+typedef struct {
+  int32_t variant;
+  uint64_t heap_bytes;
+  uint64_t max_chunks;   /* Memory::maxChunks (MemoryInitialization.cuh:161) */
+  uint64_t alloc_bytes;  /* device bytes held                                 */
+  uint64_t data_base;    /* device address of chunk 0's data (8 KiB aligned)  */
+  uint64_t data_end;
+} ouro_heap_info;
+int ouro_get_info(const ouro_heap* h, ouro_heap_info* out);
+
+/* The per-thread drop-in path, one launch of n threads (src/main.cu:10-18
+ * d_testAllocation): thread i stores malloc(size) -- or malloc(d_sizes[i]) when
+ * d_sizes is not NULL -- into d_out[i]; nullptr when out of memory. */
+int ouro_alloc(ouro_heap* h, uint32_t n, uint32_t size, const uint32_t* d_sizes, void** d_out, int block,
+               void* stream);
+
+/* src/main.cu:55-63 d_testFree: thread i frees d_ptrs[i] (nullptr is a no-op). */
+int ouro_free(ouro_heap* h, uint32_t n, void* const* d_ptrs, int block, void* stream);
+
+/* Sequential replay of an op trace by one GPU thread (threadIdx.x = tid,
+ * blockIdx.x = bid) for parity with the reference.  ops[2i] = 0: malloc(ops[2i+1]);
+ * 1: free(result of op ops[2i+1]).  results[i] (host array): class << 32 |
+ * chunk << 9 | page, bit 63 = null, bit 62 = CUDA device heap; 0 for frees.
+ * No counterpart in the reference, whose only caller is its benchmark. */
+int ouro_trace(ouro_heap* h, const uint32_t* ops, uint64_t n_ops, uint64_t* results, uint32_t tid, uint32_t bid);
+
+/* The reference's updateMemoryManagerHost (include/device/Ouroboros_impl.cuh:137-144)
+ * reduced to counters: 151 words, laid out as the oracle's state (see
+ * oracle/ouro_oracle.h).  Synchronizes the device. */
+int ouro_state(ouro_heap* h, uint64_t* out151);
+
+typedef struct {
+  uint32_t flags;             /* OURO_FLAG_*                               */
+  uint64_t null_results;      /* mallocs that returned nullptr (OOM)        */
+  uint64_t timeouts;          /* bounded waits that gave up                 */
+  uint64_t chunk_allocs;      /* chunk allocations (Statistics.h:11)        */
+  uint64_t next_free_chunk;   /* Memory::next_free_chunk                    */
+} ouro_heap_status;
+/* Device-side status; clear != 0 resets flags and counters afterwards. */
+int ouro_get_status(ouro_heap* h, ouro_heap_status* out, int clear);
+
+/* Harness kernels (src/main.cu:20-53 d_testWriteToMemory / d_testReadFromMemory
+ * with a seeded pattern): word w of allocation i holds xorshift32((i ^ seed) | 1) + w,
+ * written and checked with 16-byte vector accesses.  d_counters[0] += null
+ * pointers, d_counters[1] += mismatching words. */
+int ouro_write_pattern(void* const* d_ptrs, uint32_t n, uint32_t size, const uint32_t* d_sizes, uint32_t seed,
+                       void* stream);
+int ouro_verify_pattern(void* const* d_ptrs, uint32_t n, uint32_t size, const uint32_t* d_sizes, uint32_t seed,
+                        unsigned long long* d_counters, void* stream);
+
+/* Invariants of a set of live allocations (no counterpart in the reference):
+ * every pointer inside the heap, aligned to its size class, and no 16-byte unit
+ * owned twice (device ownership bitmap over the heap).  Synchronous. */
+typedef struct {
+  uint64_t checked;
+  uint64_t nulls;
+  uint64_t out_of_heap;
+  uint64_t misaligned;
+  uint64_t overlaps;
+} ouro_alloc_report;
+int ouro_check_allocations(ouro_heap* h, void* const* d_ptrs, uint32_t n, uint32_t size, const uint32_t* d_sizes,
+                           ouro_alloc_report* out);
+
+/* Heap accounting invariants at quiescence (no allocation in flight), per
+ * class: pages owned by the class's chunks, free pages recorded in chunk
+ * metadata, the semaphore's count / expected / reserved and the queue length.
+ * `bad` counts chunks whose count disagrees with their bitmask or whose
+ * bitmask has bits beyond its pages.  Synchronous. */
+typedef struct {
+  uint64_t owned_pages[12];
+  uint64_t free_pages_meta[12];   /* chunk-based: sum of chunk counts; page-based: queue length */
+  int64_t sem_count[12];
+  uint64_t sem_expected[12];
+  uint64_t sem_reserved[12];
+  uint64_t data_chunks;
+  uint64_t bad;
+} ouro_heap_report;
+int ouro_check_heap(ouro_heap* h, ouro_heap_report* out);
+
+const char* ouro_status_string(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

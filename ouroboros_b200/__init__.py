@@ -1,0 +1,238 @@
+"""ouroboros_b200 -- the Ouroboros device allocator, re-designed for B200.
+
+Host-side mirror of the reference's interface (GPUPeople/Ouroboros,
+include/device/Ouroboros.cuh:247-297): an :class:`Ouroboros` heap is created with
+``initialize(heap_bytes)``, its device object (``getDeviceMemoryManager()``) is
+what kernels call ``malloc``/``free`` on, and the six instantiations of
+include/InstanceDefinitions.cuh:16-34 are available under their reference names
+(``MultiOuroPQ`` ... ``MultiOuroVLCQ``).  Everything runs through the CUDA
+library ``_lib/libouroboros_b200.so`` (C ABI: include/ouroboros_b200.h); there
+is no CPU fallback -- without the library every call raises.
+
+Device buffers are passed as integers (device addresses) or torch tensors.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libouroboros_b200.so")
+
+VARIANTS = ("P", "C", "VAP", "VAC", "VLP", "VLC")
+VARIANT_NAMES = {
+    "P": "MultiOuroPQ", "C": "MultiOuroCQ", "VAP": "MultiOuroVAPQ",
+    "VAC": "MultiOuroVACQ", "VLP": "MultiOuroVLPQ", "VLC": "MultiOuroVLCQ",
+}
+STATE_WORDS = 151
+NUM_CLASSES = 12
+RES_FAIL = 1 << 63
+RES_DEVHEAP = 1 << 62
+
+FLAG_OOM, FLAG_TIMEOUT, FLAG_CORRUPT, FLAG_QUEUE_FULL = 1, 2, 4, 8
+
+# Every symbol declared in include/ouroboros_b200.h
+EXPORTS = (
+    "ouro_create", "ouro_destroy", "ouro_device_handle", "ouro_get_info", "ouro_alloc", "ouro_free",
+    "ouro_trace", "ouro_state", "ouro_get_status", "ouro_write_pattern", "ouro_verify_pattern",
+    "ouro_check_allocations", "ouro_check_heap", "ouro_status_string",
+)
+
+
+class OuroError(RuntimeError):
+    pass
+
+
+class _Info(ctypes.Structure):
+    _fields_ = [("variant", ctypes.c_int32), ("heap_bytes", ctypes.c_uint64), ("max_chunks", ctypes.c_uint64),
+                ("alloc_bytes", ctypes.c_uint64), ("data_base", ctypes.c_uint64), ("data_end", ctypes.c_uint64)]
+
+
+class _Status(ctypes.Structure):
+    _fields_ = [("flags", ctypes.c_uint32), ("null_results", ctypes.c_uint64), ("timeouts", ctypes.c_uint64),
+                ("chunk_allocs", ctypes.c_uint64), ("next_free_chunk", ctypes.c_uint64)]
+
+
+class _AllocReport(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("checked", "nulls", "out_of_heap", "misaligned", "overlaps")]
+
+
+class _HeapReport(ctypes.Structure):
+    _fields_ = [("owned_pages", ctypes.c_uint64 * 12), ("free_pages_meta", ctypes.c_uint64 * 12),
+                ("sem_count", ctypes.c_int64 * 12), ("sem_expected", ctypes.c_uint64 * 12),
+                ("sem_reserved", ctypes.c_uint64 * 12), ("data_chunks", ctypes.c_uint64), ("bad", ctypes.c_uint64)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library (raises when it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OuroError(f"{LIB_PATH} is missing: build it with `python -m ouroboros_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        p, u32, u64, i = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+        L.ouro_create.argtypes = [i, u64, ctypes.POINTER(p)]
+        L.ouro_destroy.argtypes = [p]
+        L.ouro_device_handle.argtypes = [p]
+        L.ouro_device_handle.restype = p
+        L.ouro_get_info.argtypes = [p, ctypes.POINTER(_Info)]
+        L.ouro_alloc.argtypes = [p, u32, u32, p, p, i, p]
+        L.ouro_free.argtypes = [p, u32, p, i, p]
+        L.ouro_trace.argtypes = [p, p, u64, p, u32, u32]
+        L.ouro_state.argtypes = [p, p]
+        L.ouro_get_status.argtypes = [p, ctypes.POINTER(_Status), i]
+        L.ouro_write_pattern.argtypes = [p, u32, u32, p, u32, p]
+        L.ouro_verify_pattern.argtypes = [p, u32, u32, p, u32, p, p]
+        L.ouro_check_allocations.argtypes = [p, p, u32, u32, p, ctypes.POINTER(_AllocReport)]
+        L.ouro_check_heap.argtypes = [p, ctypes.POINTER(_HeapReport)]
+        L.ouro_status_string.argtypes = [i]
+        L.ouro_status_string.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc:
+        raise OuroError(f"{what}: {lib().ouro_status_string(rc).decode()} ({rc})")
+
+
+def _addr(x) -> int | None:
+    """Device address of a tensor / int / None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x or None
+    return x.data_ptr()
+
+
+def _stream(s) -> int | None:
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return s or None
+    return s.cuda_stream or None
+
+
+class Ouroboros:
+    """One heap of one instantiation on the current device."""
+
+    def __init__(self, variant: str = "P", heap_bytes: int | None = None):
+        if variant not in VARIANTS:
+            raise ValueError(f"variant must be one of {VARIANTS}")
+        self.variant = variant
+        self._h = None
+        if heap_bytes is not None:
+            self.initialize(heap_bytes)
+
+    # -- reference interface ------------------------------------------------
+    def initialize(self, heap_bytes: int) -> "Ouroboros":
+        """Ouroboros<...>::initialize (MemoryInitialization.cuh:123-219); idempotent."""
+        if self._h is not None:
+            return self
+        h = ctypes.c_void_p()
+        _check(lib().ouro_create(VARIANTS.index(self.variant), int(heap_bytes), ctypes.byref(h)), "ouro_create")
+        self._h = h
+        return self
+
+    def getDeviceMemoryManager(self) -> int:  # noqa: N802 (reference name)
+        return int(lib().ouro_device_handle(self._handle()))
+
+    # -- lifetime -------------------------------------------------------------
+    def _handle(self):
+        if self._h is None:
+            raise OuroError("heap not initialized")
+        return self._h
+
+    def close(self):
+        if self._h is not None:
+            lib().ouro_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- launches ---------------------------------------------------------------
+    def alloc(self, out_ptrs, n: int, size: int = 0, sizes=None, block: int = 256, stream=None):
+        """Thread i of one launch: out_ptrs[i] = malloc(size or sizes[i])."""
+        _check(lib().ouro_alloc(self._handle(), n, size, _addr(sizes), _addr(out_ptrs), block, _stream(stream)),
+               "ouro_alloc")
+
+    def free(self, ptrs, n: int, block: int = 256, stream=None):
+        _check(lib().ouro_free(self._handle(), n, _addr(ptrs), block, _stream(stream)), "ouro_free")
+
+    def trace(self, ops: np.ndarray, tid: int = 0, bid: int = 0) -> np.ndarray:
+        ops = np.ascontiguousarray(ops, dtype=np.uint32)
+        res = np.zeros(ops.size // 2, dtype=np.uint64)
+        _check(lib().ouro_trace(self._handle(), ops.ctypes.data, ops.size // 2, res.ctypes.data, tid, bid),
+               "ouro_trace")
+        return res
+
+    # -- introspection --------------------------------------------------------
+    def info(self) -> dict:
+        out = _Info()
+        _check(lib().ouro_get_info(self._handle(), ctypes.byref(out)), "ouro_get_info")
+        return {n: int(getattr(out, n)) for n, _ in _Info._fields_}
+
+    def state(self) -> np.ndarray:
+        out = np.zeros(STATE_WORDS, dtype=np.uint64)
+        _check(lib().ouro_state(self._handle(), out.ctypes.data), "ouro_state")
+        return out
+
+    def status(self, clear: bool = False) -> dict:
+        out = _Status()
+        _check(lib().ouro_get_status(self._handle(), ctypes.byref(out), int(clear)), "ouro_get_status")
+        return {n: int(getattr(out, n)) for n, _ in _Status._fields_}
+
+    def check_allocations(self, ptrs, n: int, size: int = 0, sizes=None) -> dict:
+        out = _AllocReport()
+        _check(lib().ouro_check_allocations(self._handle(), _addr(ptrs), n, size, _addr(sizes), ctypes.byref(out)),
+               "ouro_check_allocations")
+        return {k: int(getattr(out, k)) for k, _ in _AllocReport._fields_}
+
+    def check_heap(self) -> dict:
+        out = _HeapReport()
+        _check(lib().ouro_check_heap(self._handle(), ctypes.byref(out)), "ouro_check_heap")
+        return {
+            "owned_pages": list(out.owned_pages), "free_pages_meta": list(out.free_pages_meta),
+            "sem_count": list(out.sem_count), "sem_expected": list(out.sem_expected),
+            "sem_reserved": list(out.sem_reserved), "data_chunks": int(out.data_chunks), "bad": int(out.bad),
+        }
+
+
+def write_pattern(ptrs, n: int, size: int = 0, seed: int = 0x9E3779B9, sizes=None, stream=None):
+    _check(lib().ouro_write_pattern(_addr(ptrs), n, size, _addr(sizes), seed & 0xFFFFFFFF, _stream(stream)),
+           "ouro_write_pattern")
+
+
+def verify_pattern(ptrs, n: int, counters, size: int = 0, seed: int = 0x9E3779B9, sizes=None, stream=None):
+    _check(lib().ouro_verify_pattern(_addr(ptrs), n, size, _addr(sizes), seed & 0xFFFFFFFF, _addr(counters),
+                                     _stream(stream)), "ouro_verify_pattern")
+
+
+def _named(variant):
+    def make(heap_bytes: int | None = None) -> Ouroboros:
+        return Ouroboros(variant, heap_bytes)
+    make.__name__ = VARIANT_NAMES[variant]
+    return make
+
+
+MultiOuroPQ = _named("P")
+MultiOuroCQ = _named("C")
+MultiOuroVAPQ = _named("VAP")
+MultiOuroVACQ = _named("VAC")
+MultiOuroVLPQ = _named("VLP")
+MultiOuroVLCQ = _named("VLC")

@@ -1,0 +1,540 @@
+// capi.cu -- host side of the B200 allocator behind the C ABI of
+// include/ouroboros_b200.h: heap creation (the reference's initialize()),
+// the per-thread launch path, sequential trace replay, state readback and the
+// invariant checkers.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/ouroboros_b200.h"
+#include "ouro/ouroboros.cuh"
+
+using namespace ouro;
+
+struct ouro_heap {
+  int variant;
+  int device;
+  unsigned long long heap_bytes;
+  Layout L;
+  void* raw;
+  HeapCore* dev;
+  char* base;
+};
+
+namespace {
+
+inline int cuda_rc(cudaError_t e) { return e == cudaSuccess ? OURO_OK : OURO_ERR_CUDA; }
+
+// ------------------------------------------------------------------ kernels
+
+// Queue initialization of the virtualized variants (MemoryInitialization.cuh:91-119
+// with PageQueueVA_impl.cuh:11-28 / PageQueueVL_impl.cuh:11-30): one queue chunk
+// per class, allocated in class order by a single thread.
+template <int V>
+__global__ void k_init_queues(Ouroboros<V>* mm) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (uint32_t cls = 0; cls < kNumClasses; ++cls) {
+    ClassState* q = &mm->cls[cls];
+    uint32_t c = new_queue_chunk(mm, q->inst, 0u);
+    if (c == kEmpty) return;
+    if constexpr (Ouroboros<V>::kKind == 1) {
+      st_relaxed(q->ring, c);
+    } else {
+      q->front_ptr = c;
+      q->back_ptr = c;
+      q->old_ptr = c;
+    }
+  }
+  __threadfence();
+}
+
+template <int V>
+__global__ void k_alloc(Ouroboros<V>* mm, uint32_t n, uint32_t size, const uint32_t* sizes, void** out) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= n) return;
+  out[tid] = mm->malloc(sizes ? sizes[tid] : size);
+}
+
+template <int V>
+__global__ void k_free(Ouroboros<V>* mm, uint32_t n, void* const* ptrs) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= n) return;
+  mm->free(ptrs[tid]);
+}
+
+// class id of the oracle's encoding: instance * 16 + queue index
+__device__ __forceinline__ uint64_t encode_result(HeapCore* h, void* p) {
+  if (!p) return 1ull << 63;
+  char* c = static_cast<char*>(p);
+  if (c < h->data || c >= h->data_end) return 1ull << 62;
+  size_t off = static_cast<size_t>(c - h->data);
+  uint32_t chunk = static_cast<uint32_t>(off >> kChunkShift);
+  uint32_t head = ld_relaxed(&h->meta[chunk].head);
+  chunk -= head;
+  uint32_t ps = ld_relaxed(&h->meta[chunk].page_size);
+  int cls = ps ? size_class(ps) : -1;
+  if (cls < 0) return (1ull << 63) | 1ull;
+  uint32_t page = static_cast<uint32_t>((off - (static_cast<size_t>(chunk) << kChunkShift)) >> class_page_shift(cls));
+  uint64_t cid = cls < 10 ? static_cast<uint64_t>(cls) : 16ull + static_cast<uint64_t>(cls - 10);
+  return (cid << 32) | mem_index(chunk, page);
+}
+
+template <int V>
+__global__ void k_trace(Ouroboros<V>* mm, const uint32_t* ops, uint64_t n, uint64_t* res, void** ptrs, uint32_t tid,
+                        uint32_t bid) {
+  if (threadIdx.x != tid || blockIdx.x != bid) return;
+  for (uint64_t i = 0; i < n; ++i) {
+    if (ops[2 * i] == 0u) {
+      void* p = mm->malloc(ops[2 * i + 1]);
+      ptrs[i] = p;
+      res[i] = encode_result(mm, p);
+    } else {
+      mm->free(ptrs[ops[2 * i + 1]]);
+      ptrs[i] = nullptr;
+      res[i] = 0;
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t pattern_seed(uint32_t i, uint32_t seed) {
+  uint32_t x = (i ^ seed) | 1u;
+  x ^= x << 13;
+  x ^= x >> 17;
+  x ^= x << 5;
+  return x;
+}
+
+// One thread per allocation, 16 B stores (pages are at least 16 B aligned).
+__global__ void k_write_pattern(void* const* ptrs, uint32_t n, uint32_t size, const uint32_t* sizes, uint32_t seed) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t* p = static_cast<uint32_t*>(ptrs[i]);
+  if (!p) return;
+  const uint32_t words = (sizes ? sizes[i] : size) / 4u;
+  const uint32_t v = pattern_seed(i, seed);
+  uint32_t w = 0;
+  for (; w + 4u <= words; w += 4u)
+    *reinterpret_cast<uint4*>(p + w) = make_uint4(v + w, v + w + 1u, v + w + 2u, v + w + 3u);
+  for (; w < words; ++w) p[w] = v + w;
+}
+
+__global__ void k_verify_pattern(void* const* ptrs, uint32_t n, uint32_t size, const uint32_t* sizes, uint32_t seed,
+                                 unsigned long long* counters) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t nulls = 0, bad = 0;
+  if (i < n) {
+    const uint32_t* p = static_cast<const uint32_t*>(ptrs[i]);
+    if (!p) {
+      nulls = 1;
+    } else {
+      const uint32_t words = (sizes ? sizes[i] : size) / 4u;
+      const uint32_t v = pattern_seed(i, seed);
+      uint32_t w = 0;
+      for (; w + 4u <= words; w += 4u) {
+        uint4 x = *reinterpret_cast<const uint4*>(p + w);
+        bad += (x.x != v + w) + (x.y != v + w + 1u) + (x.z != v + w + 2u) + (x.w != v + w + 3u);
+      }
+      for (; w < words; ++w) bad += p[w] != v + w;
+    }
+  }
+  nulls = __reduce_add_sync(0xFFFFFFFFu, nulls);
+  bad = __reduce_add_sync(0xFFFFFFFFu, bad);
+  if ((threadIdx.x & 31u) == 0u) {
+    if (nulls) atomicAdd(&counters[0], static_cast<unsigned long long>(nulls));
+    if (bad) atomicAdd(&counters[1], static_cast<unsigned long long>(bad));
+  }
+}
+
+// Ownership bitmap over the heap data at 16 B granularity.
+// r[0] checked, r[1] nulls, r[2] out of heap, r[3] misaligned, r[4] overlapping units
+__global__ void k_check_allocs(const HeapCore* h, void* const* ptrs, uint32_t n, uint32_t size, const uint32_t* sizes,
+                               uint32_t* bitmap, unsigned long long* r) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const char* p = static_cast<const char*>(ptrs[i]);
+  if (!p) { atomicAdd(&r[1], 1ull); return; }
+  atomicAdd(&r[0], 1ull);
+  const uint32_t sz = sizes ? sizes[i] : size;
+  const int cls = size_class(sz);
+  if (cls < 0) return;   // CUDA device heap
+  if (p < h->data || p + sz > h->data_end) { atomicAdd(&r[2], 1ull); return; }
+  const size_t off = static_cast<size_t>(p - h->data);
+  if (off & (class_page_size(static_cast<uint32_t>(cls)) - 1u)) atomicAdd(&r[3], 1ull);
+  const size_t u0 = off >> 4;
+  const size_t units = (sz + 15u) >> 4 ? (sz + 15u) >> 4 : 1u;
+  unsigned long long dup = 0;
+  for (size_t u = u0; u < u0 + units;) {
+    const uint32_t bit = static_cast<uint32_t>(u & 31u);
+    const uint32_t take = (32u - bit) < (u0 + units - u) ? (32u - bit) : static_cast<uint32_t>(u0 + units - u);
+    const uint32_t m = take == 32u ? 0xFFFFFFFFu : (((1u << take) - 1u) << bit);
+    const uint32_t old = atomicOr(&bitmap[u >> 5], m);
+    dup += __popc(old & m);
+    u += take;
+  }
+  if (dup) atomicAdd(&r[4], dup);
+}
+
+// Per-chunk accounting.  r layout: [0..11] owned pages, [12..23] free pages
+// (chunk counts), [24] data chunks, [25] bad chunks.
+__global__ void k_check_heap(const HeapCore* h, uint64_t nchunks, bool chunk_based, unsigned long long* r) {
+  for (uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; c < nchunks;
+       c += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const ChunkMeta* m = h->meta + c;
+    if (m->page_size == 0u || m->head != 0u) continue;
+    const int cls = size_class(m->page_size);
+    if (cls < 0) { atomicAdd(&r[25], 1ull); continue; }
+    atomicAdd(&r[24], 1ull);
+    atomicAdd(&r[cls], static_cast<unsigned long long>(m->size));
+    if (!chunk_based) continue;
+    const uint32_t words = instance_mask_words(class_instance(static_cast<uint32_t>(cls)));
+    uint32_t ones = 0, stray = 0;
+    for (uint32_t w = 0; w < words; ++w) {
+      const uint32_t lo = w * 32u;
+      const uint32_t valid = m->size >= lo + 32u ? 0xFFFFFFFFu : (m->size > lo ? ((1u << (m->size - lo)) - 1u) : 0u);
+      ones += __popc(m->mask[w] & valid);
+      stray += __popc(m->mask[w] & ~valid);
+    }
+    if (m->count >= 0) atomicAdd(&r[12 + cls], static_cast<unsigned long long>(m->count));
+    if (stray || static_cast<int32_t>(ones) != m->count) atomicAdd(&r[25], 1ull);
+  }
+}
+
+// ----------------------------------------------------------- dispatch helpers
+
+template <typename F>
+int dispatch(int variant, F&& f) {
+  switch (variant) {
+    case 0: return f(std::integral_constant<int, 0>{});
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 5: return f(std::integral_constant<int, 5>{});
+    default: return OURO_ERR_ARG;
+  }
+}
+
+inline unsigned grid_for(uint32_t n, int block) { return (n + static_cast<unsigned>(block) - 1u) / block; }
+
+bool g_heap_limit_set = false;
+
+}  // namespace
+
+extern "C" {
+
+const char* ouro_status_string(int code) {
+  switch (code) {
+    case OURO_OK: return "ok";
+    case OURO_ERR_ARG: return "bad argument";
+    case OURO_ERR_CUDA: return "CUDA runtime error";
+    case OURO_ERR_NOMEM: return "device out of memory";
+    case OURO_ERR_DEVICE: return "allocator reported an error on the device";
+    default: return "unknown status";
+  }
+}
+
+int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
+  if (!out || variant < 0 || variant > 5) return OURO_ERR_ARG;
+  *out = nullptr;
+  Layout L;
+  if (!compute_layout(variant / 2, heap_bytes, &L)) return OURO_ERR_ARG;
+  if (!g_heap_limit_set) {
+    // the reference reserves 500 MiB of CUDA device heap for requests > 32 KiB
+    // (Parameters.h:49, MemoryInitialization.cuh:130-134); only possible
+    // before the first kernel that calls device malloc
+    size_t cur = 0;
+    cudaDeviceGetLimit(&cur, cudaLimitMallocHeapSize);
+    if (cur < (500ull << 20)) cudaDeviceSetLimit(cudaLimitMallocHeapSize, 500ull << 20);
+    (void)cudaGetLastError();
+    g_heap_limit_set = true;
+  }
+  ouro_heap* h = new (std::nothrow) ouro_heap();
+  if (!h) return OURO_ERR_NOMEM;
+  h->variant = variant;
+  h->heap_bytes = heap_bytes;
+  h->L = L;
+  cudaGetDevice(&h->device);
+  if (cudaMalloc(&h->raw, L.alloc_bytes) != cudaSuccess) {
+    (void)cudaGetLastError();
+    delete h;
+    return OURO_ERR_NOMEM;
+  }
+  h->base = reinterpret_cast<char*>(align_up(reinterpret_cast<unsigned long long>(h->raw), kChunkBytes));
+  h->dev = reinterpret_cast<HeapCore*>(h->base);
+  // metadata zero, queues empty (0xFF..)
+  cudaError_t e = cudaMemset(h->base, 0, L.data_off);
+  const unsigned long long q_end = L.reuse_off + 2ull * kReuseSize * 4u;
+  if (e == cudaSuccess) e = cudaMemset(h->base + L.ring_off, 0xFF, q_end - L.ring_off);
+  HeapCore core;
+  std::memset(&core, 0, sizeof(core));
+  core.variant = variant;
+  core.max_chunks = static_cast<uint32_t>(L.max_chunks);
+  core.meta = reinterpret_cast<ChunkMeta*>(h->base + L.meta_off);
+  core.data = h->base + L.data_off;
+  core.data_end = core.data + L.max_chunks * kChunkBytes;
+  core.base = h->base;
+  core.alloc_bytes = L.alloc_bytes;
+  core.heap_bytes = heap_bytes;
+  for (int i = 0; i < 2; ++i) core.reuse[i].ring = reinterpret_cast<uint32_t*>(h->base + L.reuse_off) + i * kReuseSize;
+  const int kind = variant / 2;
+  for (uint32_t c = 0; c < kNumClasses; ++c) {
+    ClassState& q = core.cls[c];
+    q.sem.v = SemWord::kInit;
+    q.cls = c;
+    q.inst = class_instance(c);
+    q.page_size = class_page_size(c);
+    q.page_shift = class_page_shift(c);
+    q.ppc = class_pages_per_chunk(c);
+    q.words = instance_mask_words(q.inst);
+    q.front_ptr = q.back_ptr = q.old_ptr = kEmpty;
+    if (kind == 0) {
+      q.ring = reinterpret_cast<uint32_t*>(h->base + L.ring_off) + static_cast<size_t>(c) * kRingSize;
+      q.ring_mask = kRingSize - 1u;
+      q.page_cap = kRingSize;
+    } else if (kind == 1) {
+      q.ring = reinterpret_cast<uint32_t*>(h->base + L.vq_off) + static_cast<size_t>(c) * kVqSize;
+      q.ring_mask = kVqSize - 1u;
+      q.page_cap = kVqSize * kQcSpots;
+    } else {
+      q.page_cap = static_cast<uint32_t>(SemWord::kMaxCount);
+    }
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(h->base, &core, sizeof(core), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && kind != 0) {
+    dispatch(variant, [&](auto v) {
+      constexpr int V = decltype(v)::value;
+      k_init_queues<V><<<1, 32>>>(reinterpret_cast<Ouroboros<V>*>(h->dev));
+      return 0;
+    });
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    cudaFree(h->raw);
+    delete h;
+    return OURO_ERR_CUDA;
+  }
+  *out = h;
+  return OURO_OK;
+}
+
+int ouro_destroy(ouro_heap* h) {
+  if (!h) return OURO_ERR_ARG;
+  cudaError_t e = cudaFree(h->raw);
+  delete h;
+  return cuda_rc(e);
+}
+
+void* ouro_device_handle(const ouro_heap* h) { return h ? static_cast<void*>(h->dev) : nullptr; }
+
+int ouro_get_info(const ouro_heap* h, ouro_heap_info* out) {
+  if (!h || !out) return OURO_ERR_ARG;
+  out->variant = h->variant;
+  out->heap_bytes = h->heap_bytes;
+  out->max_chunks = h->L.max_chunks;
+  out->alloc_bytes = h->L.alloc_bytes;
+  out->data_base = reinterpret_cast<uint64_t>(h->base + h->L.data_off);
+  out->data_end = out->data_base + h->L.max_chunks * kChunkBytes;
+  return OURO_OK;
+}
+
+int ouro_alloc(ouro_heap* h, uint32_t n, uint32_t size, const uint32_t* d_sizes, void** d_out, int block,
+               void* stream) {
+  if (!h || !d_out || block <= 0 || block > 1024) return OURO_ERR_ARG;
+  if (n == 0) return OURO_OK;
+  return dispatch(h->variant, [&](auto v) {
+    constexpr int V = decltype(v)::value;
+    k_alloc<V><<<grid_for(n, block), block, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<Ouroboros<V>*>(h->dev), n, size, d_sizes, d_out);
+    return cuda_rc(cudaGetLastError());
+  });
+}
+
+int ouro_free(ouro_heap* h, uint32_t n, void* const* d_ptrs, int block, void* stream) {
+  if (!h || !d_ptrs || block <= 0 || block > 1024) return OURO_ERR_ARG;
+  if (n == 0) return OURO_OK;
+  return dispatch(h->variant, [&](auto v) {
+    constexpr int V = decltype(v)::value;
+    k_free<V><<<grid_for(n, block), block, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<Ouroboros<V>*>(h->dev), n, d_ptrs);
+    return cuda_rc(cudaGetLastError());
+  });
+}
+
+int ouro_trace(ouro_heap* h, const uint32_t* ops, uint64_t n_ops, uint64_t* results, uint32_t tid, uint32_t bid) {
+  if (!h || !ops || !results || n_ops == 0 || tid >= 1024u) return OURO_ERR_ARG;
+  for (uint64_t i = 0; i < n_ops; ++i) {
+    // a free must name an earlier malloc
+    if (ops[2 * i] > 1u) return OURO_ERR_ARG;
+    if (ops[2 * i] == 1u && (ops[2 * i + 1] >= i || ops[2 * ops[2 * i + 1]] != 0u)) return OURO_ERR_ARG;
+  }
+  uint32_t* d_ops = nullptr;
+  uint64_t* d_res = nullptr;
+  void** d_ptrs = nullptr;
+  if (cudaMalloc(&d_ops, 8 * n_ops) != cudaSuccess || cudaMalloc(&d_res, 8 * n_ops) != cudaSuccess ||
+      cudaMalloc(&d_ptrs, 8 * n_ops) != cudaSuccess) {
+    (void)cudaGetLastError();
+    cudaFree(d_ops);
+    cudaFree(d_res);
+    return OURO_ERR_NOMEM;
+  }
+  cudaError_t e = cudaMemcpy(d_ops, ops, 8 * n_ops, cudaMemcpyHostToDevice);
+  const uint32_t block = (tid / 32u + 1u) * 32u;
+  if (e == cudaSuccess) {
+    dispatch(h->variant, [&](auto v) {
+      constexpr int V = decltype(v)::value;
+      k_trace<V><<<bid + 1u, block>>>(reinterpret_cast<Ouroboros<V>*>(h->dev), d_ops, n_ops, d_res, d_ptrs, tid, bid);
+      return 0;
+    });
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(results, d_res, 8 * n_ops, cudaMemcpyDeviceToHost);
+  cudaFree(d_ops);
+  cudaFree(d_res);
+  cudaFree(d_ptrs);
+  return cuda_rc(e);
+}
+
+int ouro_state(ouro_heap* h, uint64_t* out) {
+  if (!h || !out) return OURO_ERR_ARG;
+  if (cudaDeviceSynchronize() != cudaSuccess) return OURO_ERR_CUDA;
+  HeapCore core;
+  if (cudaMemcpy(&core, h->dev, sizeof(core), cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
+  std::memset(out, 0, 151 * sizeof(uint64_t));
+  out[0] = core.next_free_chunk.v;
+  for (int i = 0; i < 2; ++i) {
+    out[1 + 3 * i] = static_cast<uint64_t>(static_cast<int64_t>(core.reuse[i].count.v));
+    out[2 + 3 * i] = core.reuse[i].front.v;
+    out[3 + 3 * i] = core.reuse[i].back.v;
+  }
+  const int kind = h->variant / 2;
+  const bool chunk_based = (h->variant % 2) == 1;
+  std::vector<uint32_t> vq(kVqSize);
+  for (uint32_t c = 0; c < kNumClasses; ++c) {
+    const ClassState& q = core.cls[c];
+    uint64_t* o = out + 7 + 12 * c;
+    o[0] = static_cast<uint64_t>(SemWord::count(q.sem.v));
+    o[1] = static_cast<uint64_t>(SemWord::exp_chunks(q.sem.v)) * q.ppc;
+    o[2] = SemWord::reserved(q.sem.v);
+    o[3] = q.front.v;
+    o[4] = q.back.v;
+    o[5] = chunk_based && kind != 2 ? static_cast<uint64_t>(static_cast<int64_t>(q.entries.v)) : 0u;
+    if (kind == 2) {
+      o[6] = q.front_ptr;
+      o[7] = q.back_ptr;
+      o[8] = q.old_ptr;
+      o[9] = q.old_count;
+    }
+    if (kind == 1) {
+      if (cudaMemcpy(vq.data(), q.ring, kVqSize * 4u, cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
+      uint64_t d = 0;
+      for (uint32_t v = 0; v < kVqSize; ++v)
+        if (vq[v] != kEmpty) d += static_cast<uint64_t>(v + 1u) * (static_cast<uint64_t>(vq[v]) + 1u);
+      o[10] = d;
+    }
+    o[11] = q.ppc;
+  }
+  return OURO_OK;
+}
+
+int ouro_get_status(ouro_heap* h, ouro_heap_status* out, int clear) {
+  if (!h || !out) return OURO_ERR_ARG;
+  if (cudaDeviceSynchronize() != cudaSuccess) return OURO_ERR_CUDA;
+  HeapCore core;
+  if (cudaMemcpy(&core, h->dev, sizeof(core), cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
+  out->flags = core.status.v;
+  out->null_results = core.oom.v;
+  out->timeouts = core.timeouts.v;
+  out->chunk_allocs = core.chunk_allocs.v;
+  out->next_free_chunk = core.next_free_chunk.v;
+  if (clear) {
+    const size_t off = offsetof(HeapCore, status);
+    const size_t len = offsetof(HeapCore, chunk_allocs) - off;
+    if (cudaMemset(reinterpret_cast<char*>(h->dev) + off, 0, len) != cudaSuccess) return OURO_ERR_CUDA;
+  }
+  return OURO_OK;
+}
+
+int ouro_write_pattern(void* const* d_ptrs, uint32_t n, uint32_t size, const uint32_t* d_sizes, uint32_t seed,
+                       void* stream) {
+  if (!d_ptrs) return OURO_ERR_ARG;
+  if (n == 0) return OURO_OK;
+  k_write_pattern<<<grid_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(d_ptrs, n, size, d_sizes, seed);
+  return cuda_rc(cudaGetLastError());
+}
+
+int ouro_verify_pattern(void* const* d_ptrs, uint32_t n, uint32_t size, const uint32_t* d_sizes, uint32_t seed,
+                        unsigned long long* d_counters, void* stream) {
+  if (!d_ptrs || !d_counters) return OURO_ERR_ARG;
+  if (n == 0) return OURO_OK;
+  k_verify_pattern<<<grid_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(d_ptrs, n, size, d_sizes, seed,
+                                                                                    d_counters);
+  return cuda_rc(cudaGetLastError());
+}
+
+int ouro_check_allocations(ouro_heap* h, void* const* d_ptrs, uint32_t n, uint32_t size, const uint32_t* d_sizes,
+                           ouro_alloc_report* out) {
+  if (!h || !d_ptrs || !out) return OURO_ERR_ARG;
+  const size_t units = h->L.max_chunks * (kChunkBytes / 16u);
+  const size_t words = (units + 31u) / 32u;
+  uint32_t* bitmap = nullptr;
+  unsigned long long* r = nullptr;
+  if (cudaMalloc(&bitmap, words * 4u) != cudaSuccess || cudaMalloc(&r, 5 * sizeof(unsigned long long)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    cudaFree(bitmap);
+    return OURO_ERR_NOMEM;
+  }
+  cudaError_t e = cudaMemset(bitmap, 0, words * 4u);
+  if (e == cudaSuccess) e = cudaMemset(r, 0, 5 * sizeof(unsigned long long));
+  if (e == cudaSuccess && n) {
+    k_check_allocs<<<grid_for(n, 256), 256>>>(h->dev, d_ptrs, n, size, d_sizes, bitmap, r);
+    e = cudaGetLastError();
+  }
+  unsigned long long hr[5] = {0, 0, 0, 0, 0};
+  if (e == cudaSuccess) e = cudaMemcpy(hr, r, sizeof(hr), cudaMemcpyDeviceToHost);
+  cudaFree(bitmap);
+  cudaFree(r);
+  out->checked = hr[0];
+  out->nulls = hr[1];
+  out->out_of_heap = hr[2];
+  out->misaligned = hr[3];
+  out->overlaps = hr[4];
+  return cuda_rc(e);
+}
+
+int ouro_check_heap(ouro_heap* h, ouro_heap_report* out) {
+  if (!h || !out) return OURO_ERR_ARG;
+  if (cudaDeviceSynchronize() != cudaSuccess) return OURO_ERR_CUDA;
+  HeapCore core;
+  if (cudaMemcpy(&core, h->dev, sizeof(core), cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
+  uint64_t nchunks = core.next_free_chunk.v < h->L.max_chunks ? core.next_free_chunk.v : h->L.max_chunks;
+  unsigned long long* r = nullptr;
+  if (cudaMalloc(&r, 26 * sizeof(unsigned long long)) != cudaSuccess) return OURO_ERR_NOMEM;
+  cudaError_t e = cudaMemset(r, 0, 26 * sizeof(unsigned long long));
+  const bool chunk_based = (h->variant % 2) == 1;
+  if (e == cudaSuccess && nchunks) {
+    k_check_heap<<<1184, 256>>>(h->dev, nchunks, chunk_based, r);
+    e = cudaGetLastError();
+  }
+  unsigned long long hr[26];
+  if (e == cudaSuccess) e = cudaMemcpy(hr, r, sizeof(hr), cudaMemcpyDeviceToHost);
+  cudaFree(r);
+  if (e != cudaSuccess) return OURO_ERR_CUDA;
+  for (uint32_t c = 0; c < kNumClasses; ++c) {
+    const ClassState& q = core.cls[c];
+    out->owned_pages[c] = hr[c];
+    out->free_pages_meta[c] = chunk_based ? hr[12 + c] : static_cast<uint64_t>(q.back.v - q.front.v);
+    out->sem_count[c] = SemWord::count(q.sem.v);
+    out->sem_expected[c] = static_cast<uint64_t>(SemWord::exp_chunks(q.sem.v)) * q.ppc;
+    out->sem_reserved[c] = SemWord::reserved(q.sem.v);
+  }
+  out->data_chunks = hr[24];
+  out->bad = hr[25];
+  return OURO_OK;
+}
+
+}  // extern "C"

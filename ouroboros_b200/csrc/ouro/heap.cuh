@@ -1,0 +1,238 @@
+// heap.cuh -- heap layout, chunk metadata, chunk allocation and the chunk
+// reuse queue.
+#pragma once
+
+#include "common.cuh"
+
+namespace ouro {
+
+// Out-of-band metadata of one base chunk (one 128 B line).  A chunk plays one
+// role at a time: page chunk (page-based variants), chunk-index chunk
+// (chunk-based variants: free-page count + occupancy bitmask) or queue chunk
+// (2048 queue entries of the virtualized variants, stored in its data).
+struct alignas(128) ChunkMeta {
+  uint32_t page_size;   // data chunks: page size of their class; 0 otherwise
+  uint32_t head;        // >0: continuation of a 4-chunk chunk starting `head` chunks lower
+  uint32_t size;        // pages in the chunk
+  int32_t count;        // chunk-based: free pages (may dip below 0 transiently)
+  uint32_t queue_pos;   // chunk-based: virtual position of its queue entry, kEmpty or kPending
+  uint32_t qcount;      // queue chunk: present << 16 | enqueued
+  uint32_t vstart;      // queue chunk: first virtual position stored here
+  uint32_t next;        // linked queue chunk: next queue chunk, kEmpty if none yet
+  uint32_t reserved_[8];
+  uint32_t mask[16];    // chunk-based: one bit per page, 1 = free
+};
+static_assert(sizeof(ChunkMeta) == 128, "metadata record must be one 128 B line");
+
+template <typename T>
+struct alignas(128) Line {
+  T v;
+};
+
+// Per size class queue state.  Every counter that many warps hit lives on its
+// own 128 B line so that the L2 slices serve them independently.
+struct alignas(128) ClassState {
+  Line<unsigned long long> sem;   // page semaphore (count / expected chunks / reserved)
+  Line<uint32_t> front;           // consumer position (virtual)
+  Line<uint32_t> back;            // producer position (virtual)
+  Line<int32_t> entries;          // chunk-based: entries in the queue (count_)
+  // cold line
+  uint32_t* ring;                 // standard: the ring; virtualized array: the index array
+  uint32_t ring_mask;
+  uint32_t cls, inst, page_size, page_shift, ppc, words;
+  uint32_t front_ptr, back_ptr, old_ptr, old_count;  // linked: chunk indices
+  uint32_t class_pages;           // pages ever created for the class (queue capacity guard)
+  uint32_t page_cap;
+};
+
+struct alignas(128) ReuseQueue {
+  Line<int32_t> count;
+  Line<uint32_t> front;
+  Line<uint32_t> back;
+  uint32_t* ring;
+};
+
+// Device-resident control block, the object device code calls malloc/free on.
+struct alignas(128) HeapCore {
+  // cold configuration line
+  int32_t variant;
+  uint32_t max_chunks;
+  ChunkMeta* meta;
+  char* data;
+  char* data_end;
+  char* base;
+  unsigned long long alloc_bytes;
+  unsigned long long heap_bytes;
+  // hot / warm counters
+  Line<unsigned long long> next_free_chunk;
+  Line<uint32_t> status;
+  Line<unsigned long long> oom;        // null results handed out
+  Line<unsigned long long> timeouts;   // bounded waits that gave up
+  Line<unsigned long long> chunk_allocs;
+  ReuseQueue reuse[2];
+  ClassState cls[kNumClasses];
+};
+
+constexpr size_t kCoreBytes = 16384;
+static_assert(sizeof(HeapCore) <= kCoreBytes, "control block grew past its region");
+
+__device__ __forceinline__ void set_status(HeapCore* h, uint32_t bits) { atomicOr(&h->status.v, bits); }
+__device__ __forceinline__ void note_timeout(HeapCore* h) {
+  set_status(h, kErrTimeout);
+  atomicAdd(&h->timeouts.v, 1ull);
+}
+
+// -------------------------------------------------------------- layout
+// Capacity: the reference's MemoryInitialization.cuh:156-166 arithmetic on its
+// own object and queue sizes, so that max_chunks (and with it every success /
+// failure count) is identical.  Physical placement is this build's own.
+struct Layout {
+  unsigned long long ref_queue_bytes;
+  unsigned long long ref_total_required;
+  unsigned long long max_chunks;
+  unsigned long long meta_off, data_off, ring_off, vq_off, reuse_off;
+  unsigned long long alloc_bytes;
+};
+
+__host__ __device__ inline unsigned long long align_up(unsigned long long v, unsigned long long a) {
+  return (v + a - 1u) / a * a;
+}
+
+// kind: 0 standard, 1 virtualized array, 2 virtualized linked list
+__host__ inline bool compute_layout(int kind, unsigned long long heap_bytes, Layout* L) {
+  const unsigned long long per_queue = kind == 0 ? (unsigned long long)kRingSize * 4u
+                                     : kind == 1 ? (unsigned long long)kVqSize * 4u : 0u;
+  const unsigned long long reuse = align_up((unsigned long long)kReuseSize * 4u, kChunkBytes);
+  const unsigned long long pq = align_up(per_queue, kChunkBytes);
+  L->ref_queue_bytes = reuse + pq * 10u + reuse + pq * 2u;
+  L->ref_total_required = align_up(8192u + L->ref_queue_bytes, kRefStride);
+  const unsigned long long aligned = align_up(heap_bytes, kRefStride);
+  if (aligned <= L->ref_total_required) return false;
+  L->max_chunks = (aligned - L->ref_total_required) / kRefStride;
+  if (L->max_chunks >= (1ull << (32 - kPageBits))) return false;   // MemoryIndex chunk bits
+  L->meta_off = kCoreBytes;
+  L->data_off = align_up(L->meta_off + L->max_chunks * kMetaBytes, kChunkBytes);
+  unsigned long long off = L->data_off + L->max_chunks * kChunkBytes;
+  L->ring_off = off;
+  if (kind == 0) off += (unsigned long long)kNumClasses * kRingSize * 4u;
+  L->vq_off = off;
+  if (kind == 1) off += (unsigned long long)kNumClasses * kVqSize * 4u;
+  L->reuse_off = off;
+  off += 2ull * kReuseSize * 4u;
+  L->alloc_bytes = align_up(off, kChunkBytes) + kChunkBytes;   // + slack to 8 KiB-align the base
+  return true;
+}
+
+// ------------------------------------------------------- reuse queue
+// The chunk reuse ring (queues/Queue_impl.cuh:20-66): FIFO of whole chunks
+// that left a queue.  take() serves up to k chunks for one group.
+__device__ inline uint32_t reuse_take(HeapCore* h, ReuseQueue* r, uint32_t k, uint32_t* first_pos) {
+  int32_t old = atomicSub(&r->count.v, static_cast<int32_t>(k));
+  uint32_t got = old <= 0 ? 0u : (static_cast<uint32_t>(old) < k ? static_cast<uint32_t>(old) : k);
+  if (got < k) atomicAdd(&r->count.v, static_cast<int32_t>(k - got));
+  if (got) *first_pos = atomicAdd(&r->front.v, got);
+  return got;
+}
+
+__device__ inline uint32_t reuse_read(HeapCore* h, ReuseQueue* r, uint32_t pos) {
+  uint32_t* s = r->ring + (pos & (kReuseSize - 1u));
+  uint32_t v, it = 0;
+  while ((v = ld_acquire(s)) == kEmpty) {
+    if (it >= kSpinLimit) { note_timeout(h); return kEmpty; }
+    backoff(it);
+  }
+  st_relaxed(s, kEmpty);
+  return v;
+}
+
+__device__ inline void reuse_put(HeapCore* h, ReuseQueue* r, uint32_t chunk) {
+  // a pooled chunk is nobody's data chunk: lanes that still hold a stale
+  // queue entry for it see the page size change and skip it
+  st_relaxed(&h->meta[chunk].page_size, 0u);
+  __threadfence();
+  int32_t fill = atomicAdd(&r->count.v, 1);
+  if (fill >= static_cast<int32_t>(kReuseSize)) {
+    atomicSub(&r->count.v, 1);
+    set_status(h, kErrQueueFull);   // the chunk stays out of circulation
+    return;
+  }
+  uint32_t pos = atomicAdd(&r->back.v, 1u);
+  uint32_t* s = r->ring + (pos & (kReuseSize - 1u));
+  uint32_t it = 0;
+  while (ld_relaxed(s) != kEmpty) {
+    if (it >= kSpinLimit) { note_timeout(h); return; }
+    backoff(it);
+  }
+  st_release(s, chunk);
+}
+
+// ---------------------------------------------------- chunk allocation
+// Ouroboros.cuh:108-136 / 200-229 allocateChunk, for a whole group: up to k
+// chunks (k <= group size), reuse queue first, then the bump pointer.  Lane
+// with rank i < result holds its chunk index in *mine.  A chunk is valid when
+// index + factor < max_chunks (the reference's bound).
+__device__ inline uint32_t alloc_chunks(HeapCore* h, const Group& g, uint32_t k, uint32_t inst, bool queue_chunk,
+                                        uint32_t* mine) {
+  const uint32_t factor = queue_chunk ? 1u : instance_factor(inst);
+  ReuseQueue* r = (inst != 0u && queue_chunk) ? &h->reuse[0] : &h->reuse[inst];
+  uint32_t from_reuse = 0, rpos = 0;
+  unsigned long long first = 0;
+  if (g.is_leader()) {
+    from_reuse = reuse_take(h, r, k, &rpos);
+    if (from_reuse < k) first = atomicAdd(&h->next_free_chunk.v, (unsigned long long)(k - from_reuse) * factor);
+    atomicAdd(&h->chunk_allocs.v, (unsigned long long)k);
+  }
+  from_reuse = bcast(g, from_reuse);
+  rpos = bcast(g, rpos);
+  first = bcast64(g, first);
+  uint32_t got = from_reuse;
+  const uint32_t r_ = static_cast<uint32_t>(g.rank);
+  uint32_t c = kEmpty;
+  if (r_ < from_reuse) {
+    c = reuse_read(h, r, rpos + r_);
+  } else if (r_ < k) {
+    unsigned long long idx = first + (unsigned long long)(r_ - from_reuse) * factor;
+    if (idx + factor < h->max_chunks) c = static_cast<uint32_t>(idx);
+  }
+  // bumped chunks are valid as a prefix of their range
+  unsigned long long avail = h->max_chunks > first + factor ? (h->max_chunks - first - 1u) / factor : 0u;
+  uint32_t bumped = k - from_reuse;
+  got += avail < bumped ? static_cast<uint32_t>(avail) : bumped;
+  *mine = c;
+  return got;
+}
+
+// Fresh queue chunk (QueueChunk.cuh:217-221): header reset and all 2048
+// entries set to kEmpty by the calling lane with 16 B stores.
+__device__ inline void init_queue_chunk(HeapCore* h, uint32_t c, uint32_t vstart) {
+  ChunkMeta* m = h->meta + c;
+  uint32_t* slots = reinterpret_cast<uint32_t*>(h->data + (static_cast<size_t>(c) << kChunkShift));
+  const uint4 e = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
+#pragma unroll 8
+  for (uint32_t i = 0; i < kQcSpots; i += 4u) st_v4(slots + i, e);
+  st_relaxed(&m->page_size, 0u);
+  st_relaxed(&m->head, 0u);
+  st_relaxed(&m->qcount, 0u);
+  st_relaxed(&m->vstart, vstart);
+  st_relaxed(&m->next, kEmpty);
+}
+
+__device__ __forceinline__ uint32_t* queue_slots(HeapCore* h, uint32_t c) {
+  return reinterpret_cast<uint32_t*>(h->data + (static_cast<size_t>(c) << kChunkShift));
+}
+
+// One lane allocates one queue chunk (allocateChunk<true>) and initializes it.
+__device__ inline uint32_t new_queue_chunk(HeapCore* h, uint32_t inst, uint32_t vstart) {
+  Group self = make_group(1u << lane_id());
+  uint32_t c;
+  uint32_t got = alloc_chunks(h, self, 1u, inst, true, &c);
+  if (!got || c == kEmpty) {
+    set_status(h, kErrOom);
+    return kEmpty;
+  }
+  init_queue_chunk(h, c, vstart);
+  __threadfence();
+  return c;
+}
+
+}  // namespace ouro

@@ -1,0 +1,71 @@
+// ouroboros.cuh -- the device-side allocator object.
+//
+// Ouroboros<V> is what device code holds: `mm->malloc(size)` and
+// `mm->free(ptr)` from any thread of any kernel, the interface of the
+// reference's Ouroboros<...> (Ouroboros.cuh:285-287, Ouroboros_impl.cuh:83-125).
+// V picks one of the six instantiations of InstanceDefinitions.cuh:16-34
+// (always with the second 16-32 KiB instance, as the Multi* types the
+// reference's benchmark uses):
+//   0 page-based standard (MultiOuroPQ)     1 chunk-based standard (MultiOuroCQ)
+//   2 page-based virtualized array (VAPQ)   3 chunk-based virtualized array (VACQ)
+//   4 page-based virtualized list (VLPQ)    5 chunk-based virtualized list (VLCQ)
+// Requests above 32 KiB go to the CUDA device heap, as in the reference
+// (Ouroboros.cuh:401-408).  Out of memory yields nullptr.
+#pragma once
+
+#include <type_traits>
+
+#include "queues.cuh"
+
+namespace ouro {
+
+template <int V>
+struct Ouroboros : HeapCore {
+  static_assert(V >= 0 && V < 6, "variant 0..5");
+  static constexpr bool kPageBased = (V % 2) == 0;
+  static constexpr int kKind = V / 2;
+  using Store = std::conditional_t<kKind == 0, FlatStore, std::conditional_t<kKind == 1, VaStore, VlStore>>;
+
+  __device__ __forceinline__ void* malloc(size_t size) {
+    const int cls = size_class(size);
+    const uint32_t active = __activemask();
+    const Group g = group_by(active, static_cast<uint64_t>(cls + 1));
+    if (cls < 0) {
+      // Ouroboros<>::malloc: next power of two from the CUDA device heap
+      int p2 = next_pow2_pow(size);
+      return ::malloc(static_cast<size_t>(1) << (p2 < 0 ? 0 : p2));
+    }
+    ClassState* q = &this->cls[cls];
+    if constexpr (kPageBased) return page_alloc<Store>(this, q, g);
+    else return chunk_alloc<Store>(this, q, g);
+  }
+
+  __device__ __forceinline__ void free(void* ptr) {
+    const uint32_t active = __activemask();
+    char* p = static_cast<char*>(ptr);
+    const bool in_heap = p >= this->data && p < this->data_end;
+    const uint32_t heap_mask = __ballot_sync(active, in_heap);
+    if (!in_heap) {
+      if (ptr) ::free(ptr);   // foreign pointer: the CUDA device heap (Ouroboros_impl.cuh:97-103)
+      return;
+    }
+    const size_t off = static_cast<size_t>(p - this->data);
+    uint32_t c = static_cast<uint32_t>(off >> kChunkShift);
+    uint2 ph = ld_relaxed_v2(&this->meta[c].page_size);   // page_size, head
+    if (ph.y) c -= ph.y;
+    const uint32_t page_size = ph.x;
+    int cls = page_size ? size_class(page_size) : -1;
+    const uint32_t shift = cls >= 0 ? class_page_shift(static_cast<uint32_t>(cls)) : 0u;
+    const uint32_t page = static_cast<uint32_t>((off - (static_cast<size_t>(c) << kChunkShift)) >> shift);
+    const Group g = group_by(heap_mask, static_cast<uint64_t>(cls + 1));
+    if (cls < 0) {
+      set_status(this, kErrCorrupt);
+      return;
+    }
+    ClassState* q = &this->cls[cls];
+    if constexpr (kPageBased) page_free<Store>(this, q, g, mem_index(c, page));
+    else chunk_free<Store, kKind == 0>(this, q, g, c, page);
+  }
+};
+
+}  // namespace ouro

@@ -1,0 +1,387 @@
+// queues.cuh -- page-based and chunk-based size-class queues over a storage.
+//
+// Page-based (PageQueue*_impl.cuh): the queue holds one entry per free page;
+//   a group takes g.size consecutive positions with one atomic on `front`.
+// Chunk-based (ChunkQueue*_impl.cuh): the queue holds chunks with free pages;
+//   a group scans from `front`, reserves pages on a chunk with one atomic on its
+//   count and claims bits of its occupancy mask cooperatively.
+#pragma once
+
+#include "semaphore.cuh"
+#include "store.cuh"
+
+namespace ouro {
+
+__device__ __forceinline__ void* page_address(HeapCore* h, uint32_t chunk, uint32_t page, uint32_t page_shift) {
+  return h->data + (static_cast<size_t>(chunk) << kChunkShift) + (static_cast<size_t>(page) << page_shift);
+}
+
+// Metadata of freshly allocated data chunks.  The count/mask of a chunk-index
+// chunk are written before its page size, which is what lanes validate.
+__device__ __forceinline__ void init_data_chunk(HeapCore* h, ClassState* q, uint32_t c, bool chunk_based) {
+  ChunkMeta* m = h->meta + c;
+  st_relaxed(&m->size, q->ppc);
+  st_relaxed(&m->head, 0u);
+  if (chunk_based) {
+    st_relaxed(&m->count, static_cast<int32_t>(q->ppc));
+    st_relaxed(&m->queue_pos, kEmpty);
+    // ChunkAccess.cuh:69-89: all ppc pages free
+    uint32_t n = q->ppc;
+#pragma unroll
+    for (uint32_t w = 0; w < 16u; ++w) {
+      st_relaxed(&m->mask[w], n >= 32u ? 0xFFFFFFFFu : ((1u << n) - 1u));
+      n = n > 32u ? n - 32u : 0u;
+    }
+    __threadfence();
+  }
+  st_relaxed(&m->page_size, q->page_size);
+  if (q->inst == 1u) {
+    // the three continuation chunks of a 32 KiB chunk point at their head
+    for (uint32_t k = 1; k < 4u; ++k) {
+      st_relaxed(&h->meta[c + k].head, k);
+      st_relaxed(&h->meta[c + k].page_size, q->page_size);
+    }
+  }
+}
+
+// Queue capacity guard: a class may not own more pages than its queue holds
+// (the reference traps in that case, PageQueue_impl.cuh:34).
+__device__ __forceinline__ bool reserve_class_pages(HeapCore* h, ClassState* q, uint32_t pages) {
+  uint32_t old = atomicAdd(&q->class_pages, pages);
+  if (old + pages > q->page_cap || old + pages < old) {
+    atomicSub(&q->class_pages, pages);
+    set_status(h, kErrQueueFull);
+    return false;
+  }
+  return true;
+}
+
+// ============================================================ page queues
+
+// The semaphore elected this group to add k chunks (the wait lambda of
+// PageQueue_impl.cuh:114-125): allocate, describe, publish all their pages at
+// the back with one position reservation, and credit the semaphore.
+template <class Store>
+__device__ uint32_t page_grow(HeapCore* h, ClassState* q, const Group& g, uint32_t k) {
+  uint32_t ok = 1u;
+  if (g.is_leader()) ok = reserve_class_pages(h, q, k * q->ppc) ? 1u : 0u;
+  ok = bcast(g, ok);
+  uint32_t got = 0, c = kEmpty;
+  if (ok) {
+    got = alloc_chunks(h, g, k, q->inst, false, &c);
+    if (static_cast<uint32_t>(g.rank) < got && c != kEmpty) init_data_chunk(h, q, c, false);
+    if (g.is_leader() && got < k) atomicSub(&q->class_pages, (k - got) * q->ppc);
+  }
+  const uint32_t E = got * q->ppc;
+  if (E) {
+    __threadfence();
+    uint32_t b = 0;
+    if (g.is_leader()) b = atomicAdd(&q->back.v, E);
+    b = bcast(g, b);
+    const uint32_t ppc = q->ppc;
+    Store::template publish_range<true>(h, q, g, b, E, c, ppc,
+                                        [ppc](uint32_t j, uint32_t cj) { return mem_index(cj, j % ppc); });
+    __syncwarp(g.mask);
+    __threadfence();
+  }
+  if (g.is_leader()) sem_fulfil(q, E, k);
+  return got;
+}
+
+template <class Store>
+__device__ void* page_alloc(HeapCore* h, ClassState* q, const Group& g) {
+  uint32_t granted = sem_acquire(h, q, g, [&](uint32_t k) { return page_grow<Store>(h, q, g, k); });
+  const bool served = static_cast<uint32_t>(g.rank) < granted;
+  if (granted < static_cast<uint32_t>(g.size) && g.is_leader()) {
+    atomicAdd(&h->oom.v, static_cast<unsigned long long>(g.size - granted));
+    set_status(h, kErrOom);
+  }
+  const uint32_t smask = __ballot_sync(g.mask, served);
+  if (!served) return nullptr;
+  Group s = make_group(smask);
+  uint32_t t = 0;
+  if (s.is_leader()) t = atomicAdd(&q->front.v, granted);
+  t = bcast(s, t);
+  uint32_t v = Store::consume_lane(h, q, s, t + static_cast<uint32_t>(s.rank));
+  if (v == kEmpty) return nullptr;
+  return page_address(h, v >> kPageBits, v & ((1u << kPageBits) - 1u), q->page_shift);
+}
+
+// PageQueue_impl.cuh:137-142 / PageQueueVA_impl.cuh:175-224 / PageQueueVL_impl.cuh:102-122
+template <class Store>
+__device__ void page_free(HeapCore* h, ClassState* q, const Group& g, uint32_t index) {
+  __threadfence();   // the caller's writes to the page are visible before it is handed out again
+  uint32_t b = 0;
+  if (g.is_leader()) b = atomicAdd(&q->back.v, static_cast<uint32_t>(g.size));
+  b = bcast(g, b);
+  Store::publish_lane(h, q, g, b + static_cast<uint32_t>(g.rank), index);
+  __syncwarp(g.mask);
+  __threadfence();
+  if (g.is_leader()) sem_signal(q, static_cast<uint32_t>(g.size));
+}
+
+// =========================================================== chunk queues
+
+__device__ __forceinline__ uint32_t rotr32(uint32_t m, uint32_t off) { return off ? __funnelshift_r(m, m, off) : m; }
+__device__ __forceinline__ uint32_t rotl32(uint32_t m, uint32_t off) { return off ? __funnelshift_l(m, m, off) : m; }
+
+// Entries of the chunk queue: how many, against the queue capacity.
+__device__ __forceinline__ uint32_t chunk_queue_cap(int kind) {
+  return kind == 0 ? kRingSize : kind == 1 ? kVqSize * kQcSpots : 0xFFFFFFF0u;
+}
+
+template <class Store>
+__device__ void chunk_enqueue(HeapCore* h, ClassState* q, uint32_t c) {
+  int32_t fill = atomicAdd(&q->entries.v, 1);
+  if (static_cast<uint32_t>(fill) >= chunk_queue_cap(Store::kKind)) {
+    atomicSub(&q->entries.v, 1);
+    st_relaxed(&h->meta[c].queue_pos, kEmpty);
+    set_status(h, kErrQueueFull);
+    return;
+  }
+  if (!Store::enqueue_one(h, q, c, &h->meta[c].queue_pos)) {
+    atomicSub(&q->entries.v, 1);
+    st_relaxed(&h->meta[c].queue_pos, kEmpty);
+  }
+}
+
+// A chunk whose count rose above zero must be findable: enqueue it unless it
+// still has (or is getting) an entry.  The reference does this on the first
+// free of a full chunk (ChunkQueue_impl.cuh:157-161).
+template <class Store>
+__device__ void ensure_enqueued(HeapCore* h, ClassState* q, uint32_t c) {
+  if (atomicCAS(&h->meta[c].queue_pos, kEmpty, kPending) == kEmpty) chunk_enqueue<Store>(h, q, c);
+}
+
+// Remove the entry of an exhausted chunk (the DEQUEUE_CHUNK mode of
+// ChunkQueue_impl.cuh:128-137) and advance the front over removed entries.
+template <class Store>
+__device__ void chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos) {
+  uint32_t* qp = &h->meta[c].queue_pos;
+  uint32_t it = 0;
+  while (ld_relaxed(qp) == kPending) {
+    if (it >= 4096u) return;
+    backoff(it);
+  }
+  if (atomicCAS(qp, pos, kEmpty) != pos) return;   // someone else removed or moved it
+  Store::remove(h, q, pos);
+  atomicSub(&q->entries.v, 1);
+  Store::advance_front(h, q);
+  __threadfence();
+  if (ld_relaxed(&h->meta[c].count) > 0) ensure_enqueued<Store>(h, q, c);
+}
+
+// Cooperative claim of `got` free pages of chunk c for the group lanes in
+// `want` (in rank order).  The leader picks set bits in the order the
+// reference searches them for the leader's thread (ChunkAccess_impl.cuh:75-125:
+// first word (tid + 1) mod words, bits rotated by (tid + bid) mod 32), clears
+// them with one atomicAnd per word and the group distributes the won bits.
+template <uint32_t W>
+__device__ void claim_pages(HeapCore* h, const Group& s, uint32_t c, uint32_t got, bool& served, uint32_t& page) {
+  ChunkMeta* m = h->meta + c;
+  const uint32_t start = (threadIdx.x + 1u) % W;
+  const uint32_t offset = (threadIdx.x + blockIdx.x) % 32u;
+  const uint32_t start_b = bcast(s, start);
+  const uint32_t offset_b = bcast(s, offset);
+  uint32_t remaining = got;
+  for (uint32_t attempt = 0; attempt < 64u && remaining; ++attempt) {
+    uint32_t words[W];
+    uint32_t won[W];
+    if (s.is_leader()) {
+      if constexpr (W == 16u) {
+#pragma unroll
+        for (uint32_t v = 0; v < 4u; ++v) {
+          uint4 x = ld_relaxed_v4(&m->mask[4u * v]);
+          words[4u * v] = x.x;
+          words[4u * v + 1u] = x.y;
+          words[4u * v + 2u] = x.z;
+          words[4u * v + 3u] = x.w;
+        }
+      } else {
+        words[0] = ld_relaxed(&m->mask[0]);
+      }
+      uint32_t left = remaining;
+#pragma unroll
+      for (uint32_t j = 0; j < W; ++j) {
+        const uint32_t w = (start + j) % W;
+        uint32_t word = 0u;
+#pragma unroll
+        for (uint32_t x = 0; x < W; ++x) word = x == w ? words[x] : word;
+        uint32_t rot = rotr32(word, offset);
+        uint32_t avail = __popc(rot);
+        uint32_t take = avail < left ? avail : left;
+        won[j] = 0u;
+        if (take) {
+          uint32_t p = __fns(rot, 0u, static_cast<int>(take));
+          uint32_t picked_rot = rot & ((2u << p) - 1u);
+          uint32_t picked = rotl32(picked_rot, offset);
+          uint32_t old = atomicAnd(&m->mask[w], ~picked);
+          won[j] = picked & old;
+          left -= __popc(won[j]);
+        }
+      }
+    }
+    // distribute the won bits to the unserved lanes in rank order
+    const uint32_t unserved = __ballot_sync(s.mask, !served);
+    const uint32_t u = __popc(unserved & ((1u << lane_id()) - 1u));
+    uint32_t base = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < W; ++j) {
+      uint32_t wj = __shfl_sync(s.mask, s.is_leader() ? won[j] : 0u, s.leader);
+      uint32_t cnt = __popc(wj);
+      if (!served && u >= base && u < base + cnt) {
+        uint32_t rot = rotr32(wj, offset_b);
+        uint32_t p = __fns(rot, 0u, static_cast<int>(u - base + 1u));
+        uint32_t bit = (p + offset_b) % 32u;
+        page = ((start_b + j) % W) * 32u + bit;
+        served = true;
+      }
+      base += cnt;
+    }
+    remaining -= base;
+  }
+  if (remaining && s.is_leader()) set_status(h, kErrCorrupt);   // count promised pages the mask did not show
+}
+
+// The wait lambda of ChunkQueue_impl.cuh:86-100: k empty chunks, each with one
+// queue entry, then credit the semaphore.
+template <class Store>
+__device__ uint32_t chunk_grow(HeapCore* h, ClassState* q, const Group& g, uint32_t k) {
+  uint32_t c = kEmpty;
+  uint32_t got = alloc_chunks(h, g, k, q->inst, false, &c);
+  const bool mine = static_cast<uint32_t>(g.rank) < got && c != kEmpty;
+  if (mine) {
+    init_data_chunk(h, q, c, true);
+    st_relaxed(&h->meta[c].queue_pos, kPending);
+  }
+  __syncwarp(g.mask);
+  __threadfence();
+  // one entry per chunk, in rank order (k <= group size)
+  for (uint32_t r = 0; r < got; ++r) {
+    uint32_t cr = __shfl_sync(g.mask, c, lane_of_rank(g.mask, static_cast<int>(r)));
+    if (g.is_leader() && cr != kEmpty) chunk_enqueue<Store>(h, q, cr);
+  }
+  __syncwarp(g.mask);
+  __threadfence();
+  if (g.is_leader()) sem_fulfil(q, got * q->ppc, k);
+  return got;
+}
+
+template <class Store>
+__device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
+  uint32_t granted = sem_acquire(h, q, g, [&](uint32_t k) { return chunk_grow<Store>(h, q, g, k); });
+  const bool in = static_cast<uint32_t>(g.rank) < granted;
+  if (granted < static_cast<uint32_t>(g.size) && g.is_leader()) {
+    atomicAdd(&h->oom.v, static_cast<unsigned long long>(g.size - granted));
+    set_status(h, kErrOom);
+  }
+  const uint32_t smask = __ballot_sync(g.mask, in);
+  if (!in) return nullptr;
+  Group s = make_group(smask);
+  bool served = false;
+  uint32_t page = 0, chunk = kEmpty;
+  uint32_t pos = 0;
+  typename Store::Cursor cur{};
+  if (s.is_leader()) {
+    pos = ld_relaxed(&q->front.v);
+    cur = Store::cursor(q);
+  }
+  uint32_t need = static_cast<uint32_t>(s.size);
+  uint32_t it = 0;
+  for (uint32_t iter = 0;; ++iter) {
+    uint32_t c = kEmpty, got = 0, last = 0;
+    if (s.is_leader()) {
+      if (iter > 4u * kSpinLimit) {
+        note_timeout(h);
+        c = kTomb;
+      } else {
+        uint32_t v = Store::peek(h, q, pos, cur);
+        if (v < kTomb && v < h->max_chunks && ld_relaxed(&h->meta[v].page_size) == q->page_size &&
+            ld_relaxed(&h->meta[v].count) > 0) {
+          int32_t old = atomicSub(&h->meta[v].count, static_cast<int32_t>(need));
+          got = old <= 0 ? 0u : (static_cast<uint32_t>(old) < need ? static_cast<uint32_t>(old) : need);
+          if (got < need) {
+            int32_t give = static_cast<int32_t>(need - got);
+            int32_t prev = atomicAdd(&h->meta[v].count, give);
+            if (prev <= 0 && prev + give > 0) ensure_enqueued<Store>(h, q, v);
+          }
+          last = (got > 0 && old <= static_cast<int32_t>(need)) ? 1u : 0u;
+          c = got ? v : kEmpty;
+        }
+        if (!got) {
+          // nothing here: next position; at the back, start over from the front
+          ++pos;
+          if (static_cast<int32_t>(ld_relaxed(&q->back.v) - pos) <= 0) {
+            pos = ld_relaxed(&q->front.v);
+            cur = Store::cursor(q);
+            backoff(it);
+          }
+        }
+      }
+    }
+    c = bcast(s, c);
+    if (c == kTomb) return nullptr;   // gave up
+    got = bcast(s, got);
+    if (got) {
+      last = bcast(s, last);
+      bool before = served;
+      if (q->inst == 0u) claim_pages<16u>(h, s, c, got, served, page);
+      else claim_pages<1u>(h, s, c, got, served, page);
+      if (served && !before) chunk = c;
+      if (s.is_leader()) {
+        if (last) chunk_dequeue<Store>(h, q, c, pos);
+        ++pos;
+      }
+      need = static_cast<uint32_t>(__popc(__ballot_sync(s.mask, !served)));
+      if (need == 0u) break;
+    }
+  }
+  return page_address(h, chunk, page, q->page_shift);
+}
+
+// ChunkQueue*_impl.cuh freePage: set the bits, raise the counts, re-enqueue
+// chunks that were full, then signal the semaphore once for the class group.
+template <class Store, bool Standard>
+__device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t c, uint32_t page) {
+  __threadfence();
+  Group cg = group_by(g.mask, c);
+  Group wg = group_by(cg.mask, page >> 5);
+  uint32_t bits = __reduce_or_sync(wg.mask, 1u << (page & 31u));
+  ChunkMeta* m = h->meta + c;
+  if (wg.is_leader()) atomicOr(&m->mask[page >> 5], bits);
+  __syncwarp(cg.mask);
+  __threadfence();
+  uint32_t flashed = 0;
+  if (cg.is_leader()) {
+    const int32_t n = cg.size;
+    int32_t old = atomicAdd(&m->count, n);
+    const int32_t size = static_cast<int32_t>(ld_relaxed(&m->size));
+    if (old <= 0 && old + n > 0) {
+      ensure_enqueued<Store>(h, q, c);
+    } else if (Standard && old + n == size && ld_relaxed(&q->entries.v) > kLowerFillC) {
+      // ChunkQueue_impl.cuh:162-199: hand a fully free chunk back to the pool
+      if (sem_try_reduce(q, static_cast<uint32_t>(size - n))) {
+        if (atomicCAS(&m->count, size, 0) == size) {
+          uint32_t qp, it = 0;
+          while ((qp = ld_relaxed(&m->queue_pos)) == kPending && it < 4096u) backoff(it);
+          if (qp != kPending && qp != kEmpty && atomicCAS(&m->queue_pos, qp, kEmpty) == qp) {
+            Store::remove(h, q, qp);
+            atomicSub(&q->entries.v, 1);
+            Store::advance_front(h, q);
+          }
+          reuse_put(h, &h->reuse[q->inst], c);
+          flashed = 1u;
+        } else {
+          sem_signal(q, static_cast<uint32_t>(size - n));
+        }
+      }
+    }
+  }
+  flashed = __shfl_sync(cg.mask, flashed, cg.leader);
+  __syncwarp(g.mask);
+  __threadfence();
+  uint32_t total = __reduce_add_sync(g.mask, flashed ? 0u : 1u);
+  if (g.is_leader()) sem_signal(q, total);
+}
+
+}  // namespace ouro

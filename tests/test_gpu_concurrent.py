@@ -1,0 +1,110 @@
+"""Concurrent correctness of the per-thread path: every pointer in the heap and
+aligned to its size class, no two live allocations overlapping (ownership
+bitmap + seeded pattern), and after all frees the heap accounting back at its
+idle state (every owned page free and queued, no expected or reserved pages,
+chunk bitmasks full)."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import ouroboros_b200 as ob
+
+pytestmark = pytest.mark.gpu
+
+GiB = 1 << 30
+
+
+def _ptrs(n):
+    return torch.zeros(n, dtype=torch.int64, device="cuda")
+
+
+def _idle(heap, v):
+    rep = heap.check_heap()
+    assert rep["bad"] == 0, rep
+    for c in range(12):
+        assert rep["sem_expected"][c] == 0 and rep["sem_reserved"][c] == 0, (c, rep)
+        assert rep["sem_count"][c] == rep["owned_pages"][c], (c, rep["sem_count"][c], rep["owned_pages"][c])
+        assert rep["free_pages_meta"][c] == rep["owned_pages"][c], (c, rep["free_pages_meta"][c], rep["owned_pages"][c])
+    return rep
+
+
+def _round(heap, ptrs, n, size=0, sizes=None, seed=1):
+    cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+    heap.alloc(ptrs, n, size, sizes)
+    torch.cuda.synchronize()
+    rep = heap.check_allocations(ptrs, n, size, sizes)
+    ob.write_pattern(ptrs, n, size, seed, sizes)
+    ob.verify_pattern(ptrs, n, cnt, size, seed, sizes)
+    torch.cuda.synchronize()
+    nulls, bad = cnt.tolist()
+    heap.free(ptrs, n)
+    torch.cuda.synchronize()
+    return rep, nulls, bad
+
+
+@pytest.mark.parametrize("size", [16, 64, 100, 1024, 8192, 16384, 32768])
+@pytest.mark.parametrize("v", ob.VARIANTS)
+def test_fixed_size_rounds(v, size):
+    n = 1 << 16
+    if size > 8192:
+        n = 1 << 13
+    with ob.Ouroboros(v, GiB) as heap:
+        ptrs = _ptrs(n)
+        for r in range(3):
+            rep, nulls, bad = _round(heap, ptrs, n, size, seed=r + 7)
+            assert nulls == 0 and bad == 0, (r, nulls, bad)
+            assert rep["overlaps"] == 0 and rep["misaligned"] == 0 and rep["out_of_heap"] == 0, rep
+            _idle(heap, v)
+        assert heap.status()["flags"] == 0
+
+
+@pytest.mark.parametrize("v", ob.VARIANTS)
+def test_mixed_sizes(v):
+    n = 1 << 16
+    rng = np.random.default_rng(5)
+    sizes = np.exp(rng.uniform(0, np.log(32768), n)).astype(np.uint32)
+    d_sizes = torch.from_numpy(sizes.astype(np.int32)).cuda()
+    with ob.Ouroboros(v, 2 * GiB) as heap:
+        ptrs = _ptrs(n)
+        for r in range(3):
+            rep, nulls, bad = _round(heap, ptrs, n, sizes=d_sizes, seed=r)
+            assert nulls == 0 and bad == 0, (r, nulls, bad)
+            assert rep["overlaps"] == 0 and rep["misaligned"] == 0 and rep["out_of_heap"] == 0, rep
+            _idle(heap, v)
+        assert heap.status()["flags"] == 0
+
+
+@pytest.mark.parametrize("v", ["P", "C"])
+def test_out_of_memory_exact_count(v):
+    # A heap of a few hundred chunks, asked for more 8 KiB pages than it has:
+    # exactly max_chunks - 1 requests succeed (the reference's bound
+    # index + 1 < maxChunks), the rest get nullptr; freeing restores the heap.
+    heap_bytes = oracle.layout(v, GiB)["total_required"] + 300 * 8320
+    with ob.Ouroboros(v, heap_bytes) as heap:
+        mc = heap.info()["max_chunks"]
+        n = 4096
+        ptrs = _ptrs(n)
+        for r in range(2):
+            rep, nulls, bad = _round(heap, ptrs, n, 8192, seed=r)
+            assert n - nulls == mc - 1, (n - nulls, mc)
+            assert bad == 0 and rep["overlaps"] == 0
+            _idle(heap, v)
+        st = heap.status(clear=True)
+        assert st["flags"] == ob.FLAG_OOM and st["null_results"] == 2 * (n - (mc - 1))
+
+
+@pytest.mark.parametrize("v", ["VAP", "VAC", "VLP", "VLC"])
+def test_out_of_memory_virtualized(v):
+    heap_bytes = oracle.layout(v, GiB)["total_required"] + 400 * 8320
+    with ob.Ouroboros(v, heap_bytes) as heap:
+        mc = heap.info()["max_chunks"]
+        n = 4096
+        ptrs = _ptrs(n)
+        for r in range(2):
+            rep, nulls, bad = _round(heap, ptrs, n, 8192, seed=r)
+            ok = n - nulls
+            # queue chunks come from the same pool: 12 at start plus a few
+            assert mc - 1 - 32 <= ok <= mc - 1 - 12, (ok, mc)
+            assert bad == 0 and rep["overlaps"] == 0
+        assert heap.status(clear=True)["flags"] & ~ob.FLAG_OOM == 0
