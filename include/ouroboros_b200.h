@@ -115,8 +115,9 @@ int ouro_verify_pattern(void* const* d_ptrs, uint32_t n, uint32_t size, const ui
                         unsigned long long* d_counters, void* stream);
 
 /* Invariants of a set of live allocations (no counterpart in the reference):
- * every pointer inside the heap, aligned to its size class, and no 16-byte unit
- * owned twice (device ownership bitmap over the heap).  Synchronous. */
+ * every pointer inside the heap, aligned to its size class (up to the 8 KiB
+ * chunk size: 16/32 KiB pages are 8 KiB aligned), and no 16-byte unit owned
+ * twice (device ownership bitmap over the heap).  Synchronous. */
 typedef struct {
   uint64_t checked;
   uint64_t nulls;

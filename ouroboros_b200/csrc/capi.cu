@@ -162,7 +162,11 @@ __global__ void k_check_allocs(const HeapCore* h, void* const* ptrs, uint32_t n,
   if (cls < 0) return;   // CUDA device heap
   if (p < h->data || p + sz > h->data_end) { atomicAdd(&r[2], 1ull); return; }
   const size_t off = static_cast<size_t>(p - h->data);
-  if (off & (class_page_size(static_cast<uint32_t>(cls)) - 1u)) atomicAdd(&r[3], 1ull);
+  // pages are aligned to their size class up to the 8 KiB chunk: 16/32 KiB
+  // pages sit in 4-chunk chunks that start at any chunk index
+  const uint32_t align = class_page_size(static_cast<uint32_t>(cls)) < kChunkBytes
+                             ? class_page_size(static_cast<uint32_t>(cls)) : kChunkBytes;
+  if (off & (align - 1u)) atomicAdd(&r[3], 1ull);
   const size_t u0 = off >> 4;
   const size_t units = (sz + 15u) >> 4 ? (sz + 15u) >> 4 : 1u;
   unsigned long long dup = 0;
