@@ -1,0 +1,477 @@
+#!/usr/bin/env python
+"""Alloc+free throughput of the Ouroboros allocator on B200.
+
+Workload (the all-six-instantiations configuration): every instantiation
+(P, C, VAP, VAC, VLP, VLC) on a 4 GiB heap; one launch of 2^20 threads, each
+mallocs one fixed size, then (untimed) a seeded uint32 pattern is written and
+verified, then one launch frees everything.  Sizes are the powers of two
+16 B .. 2048 B: the reference runs out of chunks at 4096 B and 8192 B
+(2^20 x 4 KiB exceeds a 4 GiB heap), so those cells are timed for this build
+only and reported under "extra".  A step is one pass over the 48 cells; the
+metric is (mallocs + frees) / (alloc kernel time + free kernel time), timed with
+CUDA events around each launch as src/main.cu:146-164 of the reference does,
+with L2 flushed (256 MiB written) before every timed launch.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference runs the reference's own CUDA code (oracle/_ref, built from the
+reference's sources for sm_100a) on the same cells, launch shape and timing.
+Under torchrun every rank runs its own replica (the allocator does not shard);
+value sums ranks over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+VARIANTS = ("P", "C", "VAP", "VAC", "VLP", "VLC")
+HEADLINE_SIZES = (16, 32, 64, 128, 256, 512, 1024, 2048)
+EXTRA_SIZES = (4096, 8192)
+GiB = 1 << 30
+SEED = 0x9E3779B9
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--variants", default=",".join(VARIANTS))
+    ap.add_argument("--sizes", default=",".join(map(str, HEADLINE_SIZES)))
+    ap.add_argument("--extra-sizes", default=",".join(map(str, EXTRA_SIZES)))
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--heap-gib", type=int, default=4)
+    ap.add_argument("--block", type=int, default=256)
+    ap.add_argument("--flush-mib", type=int, default=256)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int, enabled: bool = True):
+        self.device = device
+        self.proc = None
+        self.path = None
+        if not enabled:
+            return
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for name, val in zip(names, r[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------- the arms
+class OursArm:
+    name = "ours"
+
+    def __init__(self, heap_bytes: int):
+        import ouroboros_b200 as ob
+        self.ob = ob
+        self.heap_bytes = heap_bytes
+        self.heap = None
+
+    def open(self, v):
+        self.heap = self.ob.Ouroboros(v, self.heap_bytes)
+
+    def close(self):
+        if self.heap is not None:
+            self.heap.close()
+            self.heap = None
+
+    def alloc(self, n, size, ptrs, block, stream, sizes=None):
+        self.heap.alloc(ptrs, n, size, sizes, block, stream)
+
+    def free(self, n, ptrs, block, stream):
+        self.heap.free(ptrs, n, block, stream)
+
+    def write(self, ptrs, n, size, seed, stream):
+        self.ob.write_pattern(ptrs, n, size, seed, None, stream)
+
+    def verify(self, ptrs, n, size, seed, counters, stream):
+        self.ob.verify_pattern(ptrs, n, counters, size, seed, None, stream)
+
+    def flags(self):
+        return self.heap.status()["flags"]
+
+
+class ReferenceArm:
+    name = "reference"
+
+    def __init__(self, heap_bytes: int):
+        import oracle
+        self.oracle = oracle
+        self.heap_bytes = heap_bytes
+        self.heap = None
+
+    def open(self, v):
+        self.heap = self.oracle.RefDriver(v, self.heap_bytes)
+
+    def close(self):
+        if self.heap is not None:
+            self.heap.close()
+            self.heap = None
+
+    def alloc(self, n, size, ptrs, block, stream, sizes=None):
+        self.heap.alloc(n, size, ptrs.data_ptr(), sizes.data_ptr() if sizes is not None else 0, block,
+                        stream.cuda_stream)
+
+    def free(self, n, ptrs, block, stream):
+        self.heap.free(n, ptrs.data_ptr(), block, stream.cuda_stream)
+
+    def write(self, ptrs, n, size, seed, stream):
+        self.oracle.ref_write(ptrs.data_ptr(), n, size, seed, 0, stream.cuda_stream)
+
+    def verify(self, ptrs, n, size, seed, counters, stream):
+        self.oracle.ref_verify(ptrs.data_ptr(), n, size, seed, counters.data_ptr(), 0, stream.cuda_stream)
+
+    def flags(self):
+        return 0
+
+
+class StdoutToStderr:
+    """The reference prints banners with printf from initialize(); keep them
+    (and anything else C code writes to fd 1) off stdout, which carries only
+    the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.libc = ctypes.CDLL(None)
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        self.libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def fits_reference(v: str, size: int, n: int, heap_bytes: int) -> bool:
+    """Capacity model: chunks the cell needs against the reference's maxChunks."""
+    import oracle
+    need = -(-n * size // 8192)
+    return need + 64 < oracle.layout(v, heap_bytes)["max_chunks"]
+
+
+# ----------------------------------------------------------- measurement
+class BenchAbort(RuntimeError):
+    pass
+
+
+def run_cells(arm, cells, n, block, stream, ptrs, counters, flush, steps, warmup, e2e=False, tag="cells"):
+    """Every cell on a fresh heap (the reference benchmarks one size per process):
+    `warmup` untimed repetitions, then `steps` timed ones, each a flushed,
+    event-timed alloc launch, an untimed pattern write + verify, and a flushed,
+    event-timed free launch.  Optionally one end-to-end repetition through the
+    C ABI with host buffers.  Returns {cell: (alloc_ms list, free_ms list, e2e_ms)}."""
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    res = {}
+    if e2e:
+        sizes_h = torch.empty(n, dtype=torch.int32).pin_memory()
+        ptrs_h = torch.empty(n, dtype=torch.int64).pin_memory()
+        sizes_d = torch.empty(n, dtype=torch.int32, device="cuda")
+    for (v, size) in cells:
+        t0 = time.perf_counter()
+        arm.open(v)
+        a_ms, f_ms = [], []
+        for rep in range(warmup + steps):
+            with torch.cuda.stream(stream):
+                flush.add_(1)
+                ev[0].record(stream)
+                arm.alloc(n, size, ptrs, block, stream)
+                ev[1].record(stream)
+                arm.write(ptrs, n, size, SEED + rep, stream)
+                arm.verify(ptrs, n, size, SEED + rep, counters, stream)
+                flush.add_(1)
+                ev[2].record(stream)
+                arm.free(n, ptrs, block, stream)
+                ev[3].record(stream)
+            stream.synchronize()
+            if rep >= warmup:
+                a_ms.append(ev[0].elapsed_time(ev[1]))
+                f_ms.append(ev[2].elapsed_time(ev[3]))
+            if rep == 0:
+                flags = arm.flags()
+                if flags & ~1:
+                    arm.close()
+                    raise BenchAbort(f"device error flags {flags} after {v}:{size}")
+        e2e_ms = None
+        if e2e:
+            sizes_h.fill_(size)
+            with torch.cuda.stream(stream):
+                ev[0].record(stream)
+                sizes_d.copy_(sizes_h, non_blocking=True)
+                arm.alloc(n, 0, ptrs, block, stream, sizes=sizes_d)
+                ptrs_h.copy_(ptrs, non_blocking=True)
+                arm.free(n, ptrs, block, stream)
+                ev[1].record(stream)
+            stream.synchronize()
+            e2e_ms = ev[0].elapsed_time(ev[1])
+        flags = arm.flags()
+        arm.close()
+        if flags & ~1:
+            raise BenchAbort(f"device error flags {flags} after {v}:{size}")
+        res[(v, size)] = (a_ms, f_ms, e2e_ms)
+        print(f"[bench] {tag} {v}:{size} alloc {np.mean(a_ms):.4f} ms free {np.mean(f_ms):.4f} ms "
+              f"({time.perf_counter() - t0:.2f}s)", file=sys.stderr, flush=True)
+    return res
+
+
+def cpu_baseline(cells, n, heap_bytes) -> dict:
+    """The oracle port (one host thread) over every cell, 2^20 requests each,
+    one alloc pass and one free pass; plus glibc malloc/free on all host cores."""
+    import oracle
+    t_total, ops = 0.0, 0
+    for v, size in cells:
+        ops_arr = np.empty(4 * n, dtype=np.uint32)
+        ops_arr[0:2 * n:2] = 0
+        ops_arr[1:2 * n:2] = size
+        ops_arr[2 * n::2] = 1
+        ops_arr[2 * n + 1::2] = np.arange(n, dtype=np.uint32)
+        o = oracle.Oracle(v, heap_bytes)
+        t0 = time.perf_counter()
+        o.run_trace(ops_arr)
+        t_total += time.perf_counter() - t0
+        ops += 2 * n
+        o.close()
+    out = {"value": ops / t_total / 1e6, "unit": "Mops/s", "cores": 1, "kind": "port",
+           "sample": f"{len(cells)} cells x {n} requests, one malloc pass and one free pass each, "
+                     f"sequential C restatement of the reference (oracle/ouro_oracle.c)"}
+    so = os.path.join(ROOT, "oracle", "_build", "libhost_replay.so")
+    if os.path.exists(so):
+        lib = ctypes.CDLL(so)
+        lib.host_replay.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32,
+                                    ctypes.c_int, ctypes.c_void_p]
+        threads = os.cpu_count() or 1
+        tot, hops = 0.0, 0
+        r = np.zeros(3)
+        for v, size in cells[: len(HEADLINE_SIZES)]:
+            lib.host_replay(n, size, None, SEED, threads, r.ctypes.data)
+            tot += r[0]
+            hops += 2 * n
+        out["host_malloc"] = {"value": hops / tot / 1e6, "unit": "Mops/s", "cores": threads,
+                              "sample": f"glibc malloc/free, {len(HEADLINE_SIZES)} sizes x {n} requests "
+                                        f"(the same requests for every instantiation)"}
+    return out
+
+
+def measured_peaks() -> dict:
+    try:
+        return json.load(open(MEASURED_PEAKS))
+    except Exception:
+        return {}
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    variants = [v for v in args.variants.split(",") if v]
+    sizes = [int(s) for s in args.sizes.split(",") if s]
+    extra_sizes = [int(s) for s in args.extra_sizes.split(",") if s]
+    heap_bytes = args.heap_gib * GiB
+    n = args.n
+    cells = [(v, s) for v in variants for s in sizes]
+    stream = torch.cuda.Stream()
+    ptrs = torch.zeros(n, dtype=torch.int64, device="cuda")
+    counters = torch.zeros(2, dtype=torch.int64, device="cuda")
+    flush = torch.zeros(args.flush_mib << 18, dtype=torch.int32, device="cuda")
+
+    if args.impl == "reference":
+        import oracle
+        if not oracle.ref_available():
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libouro_ref.so was not built "
+                                  "(the reference sources were not mounted at build time)"}))
+            return 0
+        cells = [c for c in cells if fits_reference(c[0], c[1], n, heap_bytes)]
+        arm = ReferenceArm(heap_bytes)
+        extra_cells = []
+    else:
+        arm = OursArm(heap_bytes)
+        extra_cells = [(v, s) for v in variants for s in extra_sizes]
+
+    # --- timed region: every cell, W warm-up + K timed repetitions on its own heap
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local, enabled=not args.no_clocks)
+    t_wall = time.perf_counter()
+    with StdoutToStderr():
+        res = run_cells(arm, cells, n, args.block, stream, ptrs, counters, flush, args.steps, args.warmup,
+                        e2e=(args.impl == "ours" and not args.no_e2e))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    clocks = sampler.stop()
+    if dist:
+        dist.barrier()
+
+    per_cell = {}
+    total_ms = alloc_ms = free_ms = 0.0
+    e2e_ms = 0.0
+    for (v, s), (a, f, e) in res.items():
+        per_cell[f"{v}:{s}"] = {"alloc_ms": round(float(np.mean(a)), 5), "free_ms": round(float(np.mean(f)), 5),
+                                "mops": round(2.0 * n / ((np.mean(a) + np.mean(f)) * 1e-3) / 1e6, 2)}
+        total_ms += float(np.sum(a) + np.sum(f))
+        alloc_ms += float(np.sum(a))
+        free_ms += float(np.sum(f))
+        if e is not None:
+            e2e_ms += e
+    nulls, bad = counters.tolist()
+    if dist:
+        t = torch.tensor([total_ms, e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_ms = float(t[0].item()), float(t[1].item())
+    ops_total = 2.0 * n * len(cells) * args.steps * world
+    value = ops_total / (total_ms * 1e-3) / 1e6
+
+    # --- extra cells (ours only): 4096 / 8192 B exceed the heap for 2^20 requests
+    extra = {}
+    if extra_cells:
+        counters_x = torch.zeros(2, dtype=torch.int64, device="cuda")
+        try:
+            rx = run_cells(arm, extra_cells, n, args.block, stream, ptrs, counters_x, flush, 2, 1, tag="extra")
+            for (v, s), (a, f, _) in rx.items():
+                extra[f"{v}:{s}"] = {"alloc_ms": round(float(np.mean(a)), 5), "free_ms": round(float(np.mean(f)), 5)}
+            extra["null_results_per_repetition"] = int(counters_x[0].item()) // 3
+        except BenchAbort as exc:
+            extra["error"] = str(exc)
+        extra["note"] = ("2^20 x size exceeds the 4 GiB heap: the surplus requests get nullptr "
+                         "(the reference's behaviour there is undefined, it is not run)")
+
+    out = {
+        "metric": "alloc+free Mops/s (6 instantiations x 16..2048 B, 2^20 threads, 4 GiB heaps)",
+        "value": round(value, 3), "unit": "Mops/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (fixed-size requests, seeded pattern)",
+        "config": {"workload": "all six instantiations, fixed size per launch",
+                   "variants": variants, "sizes": sizes, "threads_per_launch": n, "block": args.block,
+                   "heap_bytes": heap_bytes, "cells": len(cells), "l2": f"flushed ({args.flush_mib} MiB) before every timed launch",
+                   "parallelism": f"replicas x{world}"},
+        "alloc_ms_total": round(alloc_ms, 3), "free_ms_total": round(free_ms, 3),
+        "wall_s": round(wall, 3), "null_results": nulls, "bad_words": bad,
+        "gpu_launches": 4 * len(cells) * args.steps if args.impl == "ours" else 0,
+        "timed_region": "per cell: W warm-up + K timed repetitions on a fresh heap; value = all mallocs and frees / "
+                        "summed alloc + free kernel time",
+        "clocks": clocks, "per_cell": per_cell,
+    }
+    if args.impl == "reference":
+        out["impl"] = "reference"
+        out["gpu_launches"] = 0
+        out["e2e"] = {"value": out["value"], "unit": "Mops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+        out["cpu_baseline"] = {"value": out["value"], "unit": "Mops/s", "cores": 1, "kind": "reference",
+                               "sample": "the reference's own CUDA code (sm_100a build of its sources) on the "
+                                         "same B200, the same cells, launch shape and timing; the reference "
+                                         "has no host implementation"}
+    else:
+        out["extra"] = extra
+        if e2e_ms:
+            e2e_ops = 2.0 * n * len(cells) * world
+            out["e2e"] = {"value": round(e2e_ops / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mops/s",
+                          "h2d_bytes_per_step": 4 * n * len(cells), "d2h_bytes_per_step": 8 * n * len(cells),
+                          "what": "per cell: request sizes host->device (pinned), alloc launch, pointer array "
+                                  "device->host, free launch, through the C ABI; after the timed repetitions"}
+        # roofline of the dominant kernel: the hot counters of a size class
+        import ouroboros_b200 as ob
+        hot = ob.measure_atomics(1)
+        distinct = ob.measure_atomics(0)
+        dom = "alloc" if alloc_ms >= free_ms else "free"
+        dom_ms = (alloc_ms if dom == "alloc" else free_ms) / (len(cells) * args.steps)
+        # per launch: every warp group issues one atomic on each of two counter
+        # lines (alloc: semaphore + front, free: back + semaphore)
+        requests = 2.0 * n / 32.0
+        achieved = requests / (dom_ms * 1e-3) / 1e9
+        traffic = None
+        try:
+            traffic = json.load(open(TRAFFIC_FILE)).get(f"k_{dom}")
+        except Exception:
+            pass
+        peaks = measured_peaks()
+        hbm_bytes = 16.0 * n   # per op: 8 B pointer + 4 B slot read + 4 B slot write
+        out["roofline"] = {
+            "bound": "l2_atomic", "kernel": f"k_{dom}", "achieved": round(achieved, 4),
+            "peak": round(2 * hot, 4), "unit": "G hot-counter atomics/s", "frac": round(achieved / (2 * hot), 4),
+            "traffic": traffic,
+            "peak_source": "measured live: one hot 32-bit address, one atomicAdd per warp (x2 counter lines)",
+            "distinct_address_peak_gops": round(distinct, 2),
+            "hbm": {"achieved_gbs": round(hbm_bytes / (dom_ms * 1e-3) / 1e9, 2),
+                    "peak_gbs": peaks.get("hbm_gbs"), "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+            "avg_launch_ms": round(dom_ms, 5),
+        }
+        if not args.no_cpu and rank == 0:
+            out["cpu_baseline"] = cpu_baseline(cells, n, heap_bytes)
+    if rank == 0:
+        print(json.dumps(out))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

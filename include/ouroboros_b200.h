@@ -144,6 +144,13 @@ typedef struct {
 } ouro_heap_report;
 int ouro_check_heap(ouro_heap* h, ouro_heap_report* out);
 
+/* Measured L2 atomic throughput of the current device, the roofline
+ * reference of the allocator kernels (no counterpart in the reference):
+ * mode 0 distinct addresses (atomics/s over all lanes), mode 1 one hot 32-bit
+ * address, mode 2 one hot 64-bit address (requests/s, one per warp).  Result
+ * in G operations per second. */
+int ouro_measure_atomics(int mode, double* gops);
+
 const char* ouro_status_string(int code);
 
 #ifdef __cplusplus

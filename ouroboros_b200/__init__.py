@@ -37,7 +37,7 @@ FLAG_OOM, FLAG_TIMEOUT, FLAG_CORRUPT, FLAG_QUEUE_FULL = 1, 2, 4, 8
 EXPORTS = (
     "ouro_create", "ouro_destroy", "ouro_device_handle", "ouro_get_info", "ouro_alloc", "ouro_free",
     "ouro_trace", "ouro_state", "ouro_get_status", "ouro_write_pattern", "ouro_verify_pattern",
-    "ouro_check_allocations", "ouro_check_heap", "ouro_status_string",
+    "ouro_check_allocations", "ouro_check_heap", "ouro_measure_atomics", "ouro_status_string",
 )
 
 
@@ -90,6 +90,7 @@ def lib():
         L.ouro_verify_pattern.argtypes = [p, u32, u32, p, u32, p, p]
         L.ouro_check_allocations.argtypes = [p, p, u32, u32, p, ctypes.POINTER(_AllocReport)]
         L.ouro_check_heap.argtypes = [p, ctypes.POINTER(_HeapReport)]
+        L.ouro_measure_atomics.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
         L.ouro_status_string.argtypes = [i]
         L.ouro_status_string.restype = ctypes.c_char_p
         _lib = L
@@ -221,6 +222,13 @@ def write_pattern(ptrs, n: int, size: int = 0, seed: int = 0x9E3779B9, sizes=Non
 def verify_pattern(ptrs, n: int, counters, size: int = 0, seed: int = 0x9E3779B9, sizes=None, stream=None):
     _check(lib().ouro_verify_pattern(_addr(ptrs), n, size, _addr(sizes), seed & 0xFFFFFFFF, _addr(counters),
                                      _stream(stream)), "ouro_verify_pattern")
+
+
+def measure_atomics(mode: int) -> float:
+    """G L2 atomic operations per second: 0 distinct addresses, 1 / 2 one hot 32 / 64-bit address."""
+    out = ctypes.c_double()
+    _check(lib().ouro_measure_atomics(mode, ctypes.byref(out)), "ouro_measure_atomics")
+    return float(out.value)
 
 
 def _named(variant):

@@ -46,6 +46,7 @@ __global__ void k_init_queues(Ouroboros<V>* mm) {
       q->front_ptr = c;
       q->back_ptr = c;
       q->old_ptr = c;
+      VlStore::remember(mm, q, c, 0u);
     }
   }
   __threadfence();
@@ -206,6 +207,28 @@ __global__ void k_check_heap(const HeapCore* h, uint64_t nchunks, bool chunk_bas
   }
 }
 
+
+// L2 atomic throughput references for the roofline (no counterpart in the
+// reference).  mode 0: distinct addresses, every lane one atomicAdd with return
+// on an L2-resident array; mode 1: one hot address, one atomicAdd per warp;
+// mode 2: one hot 64-bit address, one atomicAdd per warp.
+__global__ void k_peak_distinct(uint32_t* a, uint32_t mask, int iters, uint32_t* sink) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t acc = 0;
+  for (int i = 0; i < iters; ++i) acc += atomicAdd(&a[(t + static_cast<uint32_t>(i) * stride) & mask], 1u);
+  if (acc == 0x9E3779B9u) *sink = acc;
+}
+__global__ void k_peak_hot(uint32_t* a, unsigned long long* a64, int iters, int wide, uint32_t* sink) {
+  if ((threadIdx.x & 31u) != 0u) return;
+  uint32_t acc = 0;
+  for (int i = 0; i < iters; ++i) {
+    if (wide) acc += static_cast<uint32_t>(atomicAdd(a64, 32ull));
+    else acc += atomicAdd(a, 32u);
+  }
+  if (acc == 0x9E3779B9u) *sink = acc;
+}
+
 // ----------------------------------------------------------- dispatch helpers
 
 template <typename F>
@@ -268,8 +291,10 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
   }
   h->base = reinterpret_cast<char*>(align_up(reinterpret_cast<unsigned long long>(h->raw), kChunkBytes));
   h->dev = reinterpret_cast<HeapCore*>(h->base);
-  // metadata zero, queues empty (0xFF..)
+  // metadata zero; chunk data and queues flooded with kEmpty (queue chunks are
+  // taken from the data region without rewriting their entries)
   cudaError_t e = cudaMemset(h->base, 0, L.data_off);
+  if (e == cudaSuccess) e = cudaMemset(h->base + L.data_off, 0xFF, L.ring_off - L.data_off);
   const unsigned long long q_end = L.reuse_off + 2ull * kReuseSize * 4u;
   if (e == cudaSuccess) e = cudaMemset(h->base + L.ring_off, 0xFF, q_end - L.ring_off);
   HeapCore core;
@@ -294,6 +319,7 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
     q.ppc = class_pages_per_chunk(c);
     q.words = instance_mask_words(q.inst);
     q.front_ptr = q.back_ptr = q.old_ptr = kEmpty;
+    q.clean_on_recycle = (variant % 2) == 1 ? 1u : 0u;
     if (kind == 0) {
       q.ring = reinterpret_cast<uint32_t*>(h->base + L.ring_off) + static_cast<size_t>(c) * kRingSize;
       q.ring_mask = kRingSize - 1u;
@@ -304,6 +330,7 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
       q.page_cap = kVqSize * kQcSpots;
     } else {
       q.page_cap = static_cast<uint32_t>(SemWord::kMaxCount);
+      q.skip = reinterpret_cast<uint32_t*>(h->base + L.skip_off) + static_cast<size_t>(c) * kSkipSlots;
     }
   }
   if (e == cudaSuccess) e = cudaMemcpy(h->base, &core, sizeof(core), cudaMemcpyHostToDevice);
@@ -539,6 +566,41 @@ int ouro_check_heap(ouro_heap* h, ouro_heap_report* out) {
   out->data_chunks = hr[24];
   out->bad = hr[25];
   return OURO_OK;
+}
+
+
+int ouro_measure_atomics(int mode, double* gops) {
+  if (!gops || mode < 0 || mode > 2) return OURO_ERR_ARG;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  const uint32_t N = 1u << 22;   // 16 MiB: L2 resident
+  uint32_t* a = nullptr;
+  if (cudaMalloc(&a, N * 4u + 256u) != cudaSuccess) return OURO_ERR_NOMEM;
+  uint32_t* sink = a + N;
+  unsigned long long* a64 = reinterpret_cast<unsigned long long*>(a + N + 32u);
+  cudaMemset(a, 0, N * 4u + 256u);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int grid = sms * 8, block = 256;
+  const int iters = mode == 0 ? 64 : 16;
+  auto launch = [&]() {
+    if (mode == 0) k_peak_distinct<<<grid, block>>>(a, N - 1u, iters, sink);
+    else k_peak_hot<<<grid, block>>>(a, a64, iters, mode == 2, sink);
+  };
+  launch();
+  cudaEventRecord(e0);
+  for (int r = 0; r < 5; ++r) launch();
+  cudaEventRecord(e1);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  const double ops = 5.0 * grid * block * static_cast<double>(iters) / (mode == 0 ? 1.0 : 32.0);
+  *gops = ops / (ms * 1e-3) / 1e9;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(a);
+  return cuda_rc(e);
 }
 
 }  // extern "C"

@@ -31,6 +31,15 @@ constexpr uint32_t kPageBits = 9u;          // MemoryIndex page bits
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;    // free slot / no chunk
 constexpr uint32_t kTomb = 0xFFFFFFFEu;     // removed chunk-queue entry, front may pass it
 constexpr uint32_t kPending = 0xFFFFFFFEu;  // queue_pos while an enqueue is in flight
+constexpr uint32_t kInstalling = 0xFFFFFFFCu;  // queue-chunk link being installed by a waiting lane
+// A lane that waits this many polls for a queue chunk that should have been
+// pre-allocated installs one itself (the pre-allocation failed for lack of
+// chunks, or its lane is slow).
+constexpr uint32_t kInstallAfter = 256u;
+// Pooled chunks kept for queue chunks once the heap has no fresh chunk left.
+constexpr uint32_t kQueueChunkReserve = 2u * kNumClasses;
+// Slots of the linked queues' chunk index (recently linked queue chunks).
+constexpr uint32_t kSkipSlots = 1024u;
 
 // class id -> instance properties
 __host__ __device__ constexpr uint32_t class_instance(uint32_t cls) { return cls < 10u ? 0u : 1u; }

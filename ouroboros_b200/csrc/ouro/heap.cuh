@@ -43,6 +43,8 @@ struct alignas(128) ClassState {
   uint32_t front_ptr, back_ptr, old_ptr, old_count;  // linked: chunk indices
   uint32_t class_pages;           // pages ever created for the class (queue capacity guard)
   uint32_t page_cap;
+  uint32_t clean_on_recycle;      // chunk queues: queue chunks hold kTomb entries when drained
+  uint32_t* skip;                 // linked: index of recently linked queue chunks
 };
 
 struct alignas(128) ReuseQueue {
@@ -90,7 +92,7 @@ struct Layout {
   unsigned long long ref_queue_bytes;
   unsigned long long ref_total_required;
   unsigned long long max_chunks;
-  unsigned long long meta_off, data_off, ring_off, vq_off, reuse_off;
+  unsigned long long meta_off, data_off, ring_off, vq_off, skip_off, reuse_off;
   unsigned long long alloc_bytes;
 };
 
@@ -117,6 +119,8 @@ __host__ inline bool compute_layout(int kind, unsigned long long heap_bytes, Lay
   if (kind == 0) off += (unsigned long long)kNumClasses * kRingSize * 4u;
   L->vq_off = off;
   if (kind == 1) off += (unsigned long long)kNumClasses * kVqSize * 4u;
+  L->skip_off = off;
+  if (kind == 2) off += (unsigned long long)kNumClasses * kSkipSlots * 4u;
   L->reuse_off = off;
   off += 2ull * kReuseSize * 4u;
   L->alloc_bytes = align_up(off, kChunkBytes) + kChunkBytes;   // + slack to 8 KiB-align the base
@@ -126,8 +130,9 @@ __host__ inline bool compute_layout(int kind, unsigned long long heap_bytes, Lay
 // ------------------------------------------------------- reuse queue
 // The chunk reuse ring (queues/Queue_impl.cuh:20-66): FIFO of whole chunks
 // that left a queue.  take() serves up to k chunks for one group.
-__device__ inline uint32_t reuse_take(HeapCore* h, ReuseQueue* r, uint32_t k, uint32_t* first_pos) {
-  int32_t old = atomicSub(&r->count.v, static_cast<int32_t>(k));
+__device__ inline uint32_t reuse_take(HeapCore* h, ReuseQueue* r, uint32_t k, uint32_t* first_pos,
+                                      int32_t floor = 0) {
+  int32_t old = atomicSub(&r->count.v, static_cast<int32_t>(k)) - floor;
   uint32_t got = old <= 0 ? 0u : (static_cast<uint32_t>(old) < k ? static_cast<uint32_t>(old) : k);
   if (got < k) atomicAdd(&r->count.v, static_cast<int32_t>(k - got));
   if (got) *first_pos = atomicAdd(&r->front.v, got);
@@ -178,7 +183,14 @@ __device__ inline uint32_t alloc_chunks(HeapCore* h, const Group& g, uint32_t k,
   uint32_t from_reuse = 0, rpos = 0;
   unsigned long long first = 0;
   if (g.is_leader()) {
-    from_reuse = reuse_take(h, r, k, &rpos);
+    // Once the bump pointer is spent, the last few pooled chunks are kept for
+    // queue chunks: a virtualized queue that cannot grow would strand the
+    // pages already promised to it.  (Never reached below capacity, so the
+    // reuse-first order of the reference is unchanged there.)
+    int32_t floor = 0;
+    if (!queue_chunk && r == &h->reuse[0] && ld_relaxed(&h->next_free_chunk.v) + factor >= h->max_chunks)
+      floor = static_cast<int32_t>(kQueueChunkReserve);
+    from_reuse = reuse_take(h, r, k, &rpos, floor);
     if (from_reuse < k) first = atomicAdd(&h->next_free_chunk.v, (unsigned long long)(k - from_reuse) * factor);
     atomicAdd(&h->chunk_allocs.v, (unsigned long long)k);
   }
@@ -204,12 +216,14 @@ __device__ inline uint32_t alloc_chunks(HeapCore* h, const Group& g, uint32_t k,
 
 // Fresh queue chunk (QueueChunk.cuh:217-221): header reset and all 2048
 // entries set to kEmpty by the calling lane with 16 B stores.
+// Header only: the entries of a queue chunk are already kEmpty when it is
+// handed out -- the heap's data starts flooded with kEmpty (the reference's
+// d_cleanChunks, MemoryInitialization.cuh:21-38), page queues leave every
+// entry kEmpty as they drain, and chunk queues clean a queue chunk when they
+// return it to the pool (clean_queue_chunk).  This keeps the 8 KiB rewrite
+// off the path where producers wait for the next queue chunk.
 __device__ inline void init_queue_chunk(HeapCore* h, uint32_t c, uint32_t vstart) {
   ChunkMeta* m = h->meta + c;
-  uint32_t* slots = reinterpret_cast<uint32_t*>(h->data + (static_cast<size_t>(c) << kChunkShift));
-  const uint4 e = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
-#pragma unroll 8
-  for (uint32_t i = 0; i < kQcSpots; i += 4u) st_v4(slots + i, e);
   st_relaxed(&m->page_size, 0u);
   st_relaxed(&m->head, 0u);
   st_relaxed(&m->qcount, 0u);
@@ -217,19 +231,44 @@ __device__ inline void init_queue_chunk(HeapCore* h, uint32_t c, uint32_t vstart
   st_relaxed(&m->next, kEmpty);
 }
 
+// All 2048 entries of a queue chunk back to kEmpty (chunk queues leave
+// removed entries as kTomb).
+__device__ inline void clean_queue_chunk(HeapCore* h, uint32_t c) {
+  uint32_t* slots = reinterpret_cast<uint32_t*>(h->data + (static_cast<size_t>(c) << kChunkShift));
+  const uint4 e = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
+#pragma unroll 8
+  for (uint32_t i = 0; i < kQcSpots; i += 4u) st_v4(slots + i, e);
+  __threadfence();
+}
+
 __device__ __forceinline__ uint32_t* queue_slots(HeapCore* h, uint32_t c) {
   return reinterpret_cast<uint32_t*>(h->data + (static_cast<size_t>(c) << kChunkShift));
 }
 
 // One lane allocates one queue chunk (allocateChunk<true>) and initializes it.
+__device__ inline uint32_t new_queue_chunk(HeapCore* h, uint32_t inst, uint32_t vstart);
+
+// Link slot of a queue chunk (a virtual-array index entry or a `next` field):
+// the pre-allocating lane offers its chunk with a CAS; if a waiting lane got
+// there first the offered chunk goes back to the pool.
+__device__ inline void offer_queue_chunk(HeapCore* h, uint32_t* link, uint32_t nq) {
+  if (nq == kEmpty) return;
+  if (atomicCAS(link, kEmpty, nq) != kEmpty) reuse_put(h, &h->reuse[0], nq);
+}
+
+// A lane that has waited long for a link installs a queue chunk itself.
+// Returns true when the link is now set (by anyone).
+__device__ inline void install_queue_chunk(HeapCore* h, uint32_t* link, uint32_t inst, uint32_t vstart) {
+  if (atomicCAS(link, kEmpty, kInstalling) != kEmpty) return;
+  uint32_t nq = new_queue_chunk(h, inst, vstart);
+  st_release(link, nq);   // kEmpty again when no chunk was free: someone retries later
+}
+
 __device__ inline uint32_t new_queue_chunk(HeapCore* h, uint32_t inst, uint32_t vstart) {
   Group self = make_group(1u << lane_id());
   uint32_t c;
   uint32_t got = alloc_chunks(h, self, 1u, inst, true, &c);
-  if (!got || c == kEmpty) {
-    set_status(h, kErrOom);
-    return kEmpty;
-  }
+  if (!got || c == kEmpty) return kEmpty;
   init_queue_chunk(h, c, vstart);
   __threadfence();
   return c;

@@ -287,7 +287,8 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
     cur = Store::cursor(q);
   }
   uint32_t need = static_cast<uint32_t>(s.size);
-  uint32_t it = 0;
+  uint32_t it = 0, misses = 0, tombs = 0;
+  uint32_t rng = (blockIdx.x * 32u + threadIdx.x / 32u) * 2654435761u + 12345u;
   for (uint32_t iter = 0;; ++iter) {
     uint32_t c = kEmpty, got = 0, last = 0;
     if (s.is_leader()) {
@@ -296,8 +297,16 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
         c = kTomb;
       } else {
         uint32_t v = Store::peek(h, q, pos, cur);
-        if (v < kTomb && v < h->max_chunks && ld_relaxed(&h->meta[v].page_size) == q->page_size &&
-            ld_relaxed(&h->meta[v].count) > 0) {
+        if (v == kTomb && ++tombs >= 4u) {
+          // removed entries ahead of us: help the front past them and skip
+          tombs = 0;
+          Store::advance_front(h, q);
+          const uint32_t f = ld_relaxed(&q->front.v);
+          if (static_cast<int32_t>(f - pos) > 0) pos = f;
+        }
+        const bool live = v < kTomb && v < h->max_chunks && ld_relaxed(&h->meta[v].page_size) == q->page_size;
+        if (live && ld_relaxed(&h->meta[v].count) <= 0) ++misses;
+        if (live && ld_relaxed(&h->meta[v].count) > 0) {
           int32_t old = atomicSub(&h->meta[v].count, static_cast<int32_t>(need));
           got = old <= 0 ? 0u : (static_cast<uint32_t>(old) < need ? static_cast<uint32_t>(old) : need);
           if (got < need) {
@@ -309,12 +318,24 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
           c = got ? v : kEmpty;
         }
         if (!got) {
+          if (live) ++misses;
           // nothing here: next position; at the back, start over from the front
           ++pos;
-          if (static_cast<int32_t>(ld_relaxed(&q->back.v) - pos) <= 0) {
+          const uint32_t back = ld_relaxed(&q->back.v);
+          if (static_cast<int32_t>(back - pos) <= 0) {
             pos = ld_relaxed(&q->front.v);
             cur = Store::cursor(q);
             backoff(it);
+          } else if (misses >= 2u) {
+            // Many groups scan from the same front; after two exhausted
+            // chunks jump to a random position of the remaining window.  A
+            // lone lane never misses (exhausted chunks leave the queue at
+            // once), so it keeps the reference's front-first order.
+            misses = 0;
+            rng = rng * 1664525u + 1013904223u;
+            uint32_t front = ld_relaxed(&q->front.v);
+            if (static_cast<int32_t>(pos - front) < 0) pos = front;
+            pos += (rng >> 8) % (back - pos);
           }
         }
       }

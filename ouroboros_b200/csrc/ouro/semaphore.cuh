@@ -129,8 +129,11 @@ __device__ inline uint32_t sem_acquire(HeapCore* h, ClassState* q, const Group& 
             }
             unsigned long long seen = atomicCAS(&q->sem.v, v, nv);
             if (seen == v) break;
-            v = seen;
             if (tries > kSpinLimit) { note_timeout(h); mode = kFail; break; }
+            // contended: back off before re-reading, so that thousands of
+            // arriving warps do not turn the word into a CAS storm
+            __nanosleep(16u << (tries < 6u ? tries : 6u));
+            v = ld_relaxed(&q->sem.v);
           }
           if (mode == kReserve) {
             // wait until the pages are there or our reservation is no longer covered

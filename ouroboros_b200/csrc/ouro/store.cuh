@@ -93,14 +93,22 @@ struct FlatStore {
   __device__ static void remove(HeapCore* h, ClassState* q, uint32_t pos) { st_relaxed(slot(q, pos), kTomb); }
 
   // Move the front past removed entries, freeing their slots for the next lap.
+  // The removed run is found with plain loads and claimed with one CAS, so
+  // many lanes finishing chunks at once do not fight over the front word.
   __device__ static void advance_front(HeapCore* h, ClassState* q) {
-    for (uint32_t i = 0; i < 64u; ++i) {
-      uint32_t f = ld_relaxed(&q->front.v);
-      if (static_cast<int32_t>(ld_relaxed(&q->back.v) - f) <= 0) return;
-      uint32_t* s = slot(q, f);
-      if (ld_relaxed(s) != kTomb) return;
-      if (atomicCAS(&q->front.v, f, f + 1u) == f) st_relaxed(s, kEmpty);
+    const uint32_t f = ld_relaxed(&q->front.v);
+    const uint32_t back = ld_relaxed(&q->back.v);
+    uint32_t g = f;
+    while (g != back && g - f < 4096u && ld_relaxed(slot(q, g)) == kTomb) ++g;
+    if (g == f) return;
+    uint32_t cur = f;
+    for (;;) {
+      const uint32_t seen = atomicCAS(&q->front.v, cur, g);
+      if (seen == cur) break;
+      if (static_cast<int32_t>(seen - g) >= 0) return;   // someone else moved it at least as far
+      cur = seen;                                         // [seen, g) is still ours to pass
     }
+    for (uint32_t p = cur; p != g; ++p) st_relaxed(slot(q, p), kEmpty);
   }
 };
 
@@ -114,8 +122,10 @@ struct VaStore {
   __device__ static uint32_t qchunk(HeapCore* h, ClassState* q, uint32_t pos) {
     uint32_t* e = q->ring + vid(pos);
     uint32_t c, it = 0;
-    while ((c = ld_acquire(e)) == kEmpty) {
+    while ((c = ld_acquire(e)) == kEmpty || c == kInstalling) {
       if (it >= kSpinLimit) { note_timeout(h); return kEmpty; }
+      if (c == kEmpty && it >= kInstallAfter && (it & 63u) == 0u)
+        install_queue_chunk(h, e, q->inst, pos - pos % kQcSpots);
       backoff(it);
     }
     if (ld_relaxed(&h->meta[c].vstart) / kQcSpots != pos / kQcSpots) {
@@ -128,14 +138,13 @@ struct VaStore {
   // The producer of a position at the start of a queue chunk allocates the
   // next queue chunk (PageQueueVA_impl.cuh:45-56, :202-212).
   __device__ static void preallocate(HeapCore* h, ClassState* q, uint32_t pos) {
-    uint32_t nq = new_queue_chunk(h, q->inst, pos + kQcSpots);
-    if (nq != kEmpty) st_release(q->ring + vid(pos + kQcSpots), nq);
+    offer_queue_chunk(h, q->ring + vid(pos + kQcSpots), new_queue_chunk(h, q->inst, pos + kQcSpots));
   }
 
   // Drained queue chunk back to the chunk pool (PageQueueVA_impl.cuh:159-166).
   __device__ static void recycle(HeapCore* h, ClassState* q, uint32_t pos) {
     uint32_t c = atomicExch(q->ring + vid(pos), kEmpty);
-    if (c != kEmpty) reuse_put(h, &h->reuse[0], c);
+    if (c < kInstalling) reuse_put(h, &h->reuse[0], c);
   }
 
   // Count update of a range: m entries enqueued into the chunk of pos.
@@ -143,6 +152,15 @@ struct VaStore {
     uint32_t add = (m << 16) + m;
     uint32_t old = atomicAdd(&h->meta[c].qcount, add);
     if (recycle_ok && old + add == kQcSpots) recycle(h, q, pos);
+  }
+
+  // The lanes of a group hold contiguous positions that span at most two
+  // queue chunks.  Each half is written and counted on its own, so the count
+  // of the first chunk never waits for the second chunk to appear.
+  __device__ static Group half_of(const Group& g, uint32_t pos, uint32_t first) {
+    const bool second = pos / kQcSpots != first / kQcSpots;
+    const uint32_t m2 = __ballot_sync(g.mask, second);
+    return make_group(second ? m2 : (g.mask & ~m2));
   }
 
   template <bool PageQueue, typename Value>
@@ -154,54 +172,56 @@ struct VaStore {
       uint32_t j = static_cast<uint32_t>(g.rank) + i * n;
       if (j < E && ((b + j) % kQcSpots) == 0u) preallocate(h, q, b + j);
     }
-    uint32_t c1 = kEmpty, c2 = kEmpty;
-    const uint32_t split = kQcSpots - (b % kQcSpots);   // entries that land in the first queue chunk
-    for (uint32_t i = 0; i < rounds; ++i) {
-      uint32_t j = static_cast<uint32_t>(g.rank) + i * n;
-      int src = j < E ? lane_of_rank(g.mask, static_cast<int>(j / entries_per_chunk)) : g.leader;
-      uint32_t cj = __shfl_sync(g.mask, chunk, src);
-      if (j < E) {
-        uint32_t p = b + j;
-        uint32_t qc = qchunk(h, q, p);
-        if (qc == kEmpty) continue;
-        if (j < split) c1 = qc; else c2 = qc;
-        uint32_t* s = queue_slots(h, qc) + (p % kQcSpots);
-        if (wait_slot_empty(h, s)) st_relaxed(s, value(j, cj));
+    const uint32_t room = kQcSpots - (b % kQcSpots);
+    const uint32_t split = E < room ? E : room;
+    for (uint32_t half = 0; half < 2u; ++half) {
+      const uint32_t j0 = half ? split : 0u, j1 = half ? E : split;
+      if (j0 >= j1) continue;
+      uint32_t qc = kEmpty;
+      if (g.is_leader()) qc = qchunk(h, q, b + j0);
+      qc = bcast(g, qc);
+      if (qc == kEmpty) continue;
+      const uint32_t r2 = (j1 - j0 + n - 1u) / n;
+      for (uint32_t i = 0; i < r2; ++i) {
+        uint32_t j = j0 + static_cast<uint32_t>(g.rank) + i * n;
+        int src = j < j1 ? lane_of_rank(g.mask, static_cast<int>(j / entries_per_chunk)) : g.leader;
+        uint32_t cj = __shfl_sync(g.mask, chunk, src);
+        if (j < j1) {
+          uint32_t* s = queue_slots(h, qc) + ((b + j) % kQcSpots);
+          if (wait_slot_empty(h, s)) st_relaxed(s, value(j, cj));
+        }
       }
-    }
-    __syncwarp(g.mask);
-    __threadfence();
-    // the leader may not have touched both chunks: take them from any lane
-    c1 = __reduce_min_sync(g.mask, c1);
-    c2 = __reduce_min_sync(g.mask, c2);
-    if (g.is_leader()) {
-      uint32_t m1 = E < split ? E : split;
-      if (c1 != kEmpty && m1) count_enqueued(h, q, c1, b, m1, PageQueue);
-      if (c2 != kEmpty && E > m1) count_enqueued(h, q, c2, b + m1, E - m1, PageQueue);
+      __syncwarp(g.mask);
+      __threadfence();
+      if (g.is_leader()) count_enqueued(h, q, qc, b + j0, j1 - j0, PageQueue);
     }
   }
 
   __device__ static void publish_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos, uint32_t v) {
+    const Group sg = half_of(g, pos, bcast(g, pos));
     if (pos % kQcSpots == 0u) preallocate(h, q, pos);
-    uint32_t qc = qchunk(h, q, pos);
+    uint32_t qc = kEmpty;
+    if (sg.is_leader()) qc = qchunk(h, q, pos);
+    qc = bcast(sg, qc);
     if (qc != kEmpty) {
       uint32_t* s = queue_slots(h, qc) + (pos % kQcSpots);
       if (wait_slot_empty(h, s)) st_relaxed(s, v);
     }
-    __syncwarp(g.mask);
+    __syncwarp(sg.mask);
     __threadfence();
-    Group cg = group_by(g.mask, qc);
-    if (cg.is_leader() && qc != kEmpty) count_enqueued(h, q, qc, pos, static_cast<uint32_t>(cg.size), true);
+    if (sg.is_leader() && qc != kEmpty) count_enqueued(h, q, qc, pos, static_cast<uint32_t>(sg.size), true);
   }
 
   __device__ static uint32_t consume_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos) {
-    uint32_t qc = qchunk(h, q, pos);
+    const Group sg = half_of(g, pos, bcast(g, pos));
+    uint32_t qc = kEmpty;
+    if (sg.is_leader()) qc = qchunk(h, q, pos);
+    qc = bcast(sg, qc);
     uint32_t v = kEmpty;
     if (qc != kEmpty) v = take_slot(h, queue_slots(h, qc) + (pos % kQcSpots));
-    __syncwarp(g.mask);
-    Group cg = group_by(g.mask, qc);
-    if (cg.is_leader() && qc != kEmpty) {
-      uint32_t sub = static_cast<uint32_t>(cg.size) << 16;
+    __syncwarp(sg.mask);
+    if (sg.is_leader() && qc != kEmpty) {
+      uint32_t sub = static_cast<uint32_t>(sg.size) << 16;
       uint32_t old = atomicSub(&h->meta[qc].qcount, sub);
       if (old - sub == kQcSpots) recycle(h, q, pos);
     }
@@ -226,28 +246,45 @@ struct VaStore {
   __device__ static Cursor cursor(ClassState*) { return Cursor{0}; }
   __device__ static uint32_t peek(HeapCore* h, ClassState* q, uint32_t pos, Cursor&) {
     uint32_t qc = ld_acquire(q->ring + vid(pos));
-    if (qc == kEmpty) return kEmpty;
+    if (qc >= kInstalling) return kEmpty;
     if (ld_relaxed(&h->meta[qc].vstart) / kQcSpots != pos / kQcSpots) return kTomb;
     return ld_acquire(queue_slots(h, qc) + (pos % kQcSpots));
   }
   __device__ static void remove(HeapCore* h, ClassState* q, uint32_t pos) {
     uint32_t qc = ld_acquire(q->ring + vid(pos));
-    if (qc == kEmpty) return;
+    if (qc >= kInstalling) return;
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
     atomicSub(&h->meta[qc].qcount, 1u << 16);
   }
   // Front moves over removed entries; passing the last entry of a queue chunk
-  // returns that chunk to the pool (ChunkQueueVA_impl.cuh:144-156).
+  // returns that chunk to the pool (ChunkQueueVA_impl.cuh:144-156).  Same
+  // scan-then-one-CAS scheme as the flat ring.
   __device__ static void advance_front(HeapCore* h, ClassState* q) {
-    for (uint32_t i = 0; i < 64u; ++i) {
-      uint32_t f = ld_relaxed(&q->front.v);
-      if (static_cast<int32_t>(ld_relaxed(&q->back.v) - f) <= 0) return;
-      uint32_t qc = ld_acquire(q->ring + vid(f));
-      if (qc == kEmpty) return;
-      if (ld_acquire(queue_slots(h, qc) + (f % kQcSpots)) != kTomb) return;
-      if (atomicCAS(&q->front.v, f, f + 1u) == f && ((f + 1u) % kQcSpots) == 0u) {
-        uint32_t c = atomicExch(q->ring + vid(f), kEmpty);
-        if (c != kEmpty) reuse_put(h, &h->reuse[0], c);
+    const uint32_t f = ld_relaxed(&q->front.v);
+    const uint32_t back = ld_relaxed(&q->back.v);
+    uint32_t g = f, qc = kEmpty;
+    while (g != back && g - f < 4096u) {
+      if (g == f || g % kQcSpots == 0u) {
+        qc = ld_acquire(q->ring + vid(g));
+        if (qc >= kInstalling || ld_relaxed(&h->meta[qc].vstart) / kQcSpots != g / kQcSpots) break;
+      }
+      if (ld_acquire(queue_slots(h, qc) + (g % kQcSpots)) != kTomb) break;
+      ++g;
+    }
+    if (g == f) return;
+    uint32_t cur = f;
+    for (;;) {
+      const uint32_t seen = atomicCAS(&q->front.v, cur, g);
+      if (seen == cur) break;
+      if (static_cast<int32_t>(seen - g) >= 0) return;
+      cur = seen;
+    }
+    // every queue chunk whose last entry lies in [cur, g) is now behind the front
+    for (uint32_t end = cur - cur % kQcSpots + kQcSpots; static_cast<int32_t>(g - end) >= 0; end += kQcSpots) {
+      const uint32_t c = atomicExch(q->ring + vid(end - 1u), kEmpty);
+      if (c < kInstalling) {
+        clean_queue_chunk(h, c);
+        reuse_put(h, &h->reuse[0], c);
       }
     }
   }
@@ -258,6 +295,18 @@ struct VlStore {
   static constexpr int kKind = 2;
   static constexpr uint32_t kBehind = 0xFFFFFFFDu;
 
+  // Direct-mapped index of recently linked queue chunks (virtual chunk id mod
+  // kSkipSlots).  An entry is only a hint, valid when the chunk's vstart
+  // matches; it turns the pointer chase of a burst into one lookup.
+  __device__ static void remember(HeapCore* h, ClassState* q, uint32_t c, uint32_t vstart) {
+    st_relaxed(q->skip + ((vstart / kQcSpots) & (kSkipSlots - 1u)), c);
+  }
+  __device__ static uint32_t recall(HeapCore* h, ClassState* q, uint32_t pos) {
+    const uint32_t c = ld_relaxed(q->skip + ((pos / kQcSpots) & (kSkipSlots - 1u)));
+    if (c < h->max_chunks && ld_relaxed(&h->meta[c].vstart) / kQcSpots == pos / kQcSpots) return c;
+    return kEmpty;
+  }
+
   // Walk from `from` to the queue chunk holding pos (QueueChunk_impl.cuh:403-426).
   // Returns kBehind when pos precedes `from`, kEmpty on timeout.
   __device__ static uint32_t locate(HeapCore* h, uint32_t from, uint32_t pos) {
@@ -267,30 +316,47 @@ struct VlStore {
       uint32_t want = pos / kQcSpots;
       if (vs == want) return cur;
       if (static_cast<int32_t>(want - vs) < 0) return kBehind;
-      uint32_t nx;
-      while ((nx = ld_acquire(&h->meta[cur].next)) == kEmpty) {
-        if (it >= kSpinLimit) { note_timeout(h); return kEmpty; }
-        backoff(it);
-      }
+      uint32_t nx = next_of(h, cur, it);
+      if (nx == kEmpty) return kEmpty;
       cur = nx;
     }
     note_timeout(h);
     return kEmpty;
   }
 
-  __device__ static uint32_t next_of(HeapCore* h, uint32_t c) {
-    uint32_t nx, it = 0;
-    while ((nx = ld_acquire(&h->meta[c].next)) == kEmpty) {
+  // locate() for a position the caller holds (its queue chunk cannot drain
+  // meanwhile), trying the index first.
+  __device__ static uint32_t locate_live(HeapCore* h, ClassState* q, uint32_t from, uint32_t pos) {
+    const uint32_t c = recall(h, q, pos);
+    return c != kEmpty ? c : locate(h, from, pos);
+  }
+
+  // The queue chunk after c, waiting for its link (and installing one when
+  // the pre-allocation does not show up).  Only called for positions that a
+  // producer has already reserved, so the link must come.
+  __device__ static uint32_t next_of(HeapCore* h, uint32_t c, uint32_t& it) {
+    uint32_t* link = &h->meta[c].next;
+    uint32_t nx;
+    while ((nx = ld_acquire(link)) == kEmpty || nx == kInstalling) {
       if (it >= kSpinLimit) { note_timeout(h); return kEmpty; }
+      if (nx == kEmpty && it >= kInstallAfter && (it & 63u) == 0u) {
+        uint32_t vs = ld_relaxed(&h->meta[c].vstart);
+        install_queue_chunk(h, link, 0u, vs - vs % kQcSpots + kQcSpots);   // queue chunks always come from the base pool
+      }
       backoff(it);
     }
     return nx;
   }
+  __device__ static uint32_t next_of(HeapCore* h, uint32_t c) {
+    uint32_t it = 0;
+    return next_of(h, c, it);
+  }
 
-  // QueueChunk_impl.cuh:440-463 setBackPointer
+  // QueueChunk_impl.cuh:440-463 setBackPointer.  Called when cur is full, so
+  // its link exists or is about to (its first producer pre-allocates it).
   __device__ static void set_back(HeapCore* h, ClassState* q, uint32_t cur) {
     for (uint32_t i = 0; i < (1u << 16); ++i) {
-      uint32_t nx = ld_acquire(&h->meta[cur].next);
+      uint32_t nx = next_of(h, cur);
       if (nx == kEmpty) return;
       if (atomicCAS(&q->back_ptr, cur, nx) != cur) return;
       if ((ld_relaxed(&h->meta[nx].qcount) & 0xFFFFu) == kQcSpots) cur = nx;
@@ -302,7 +368,7 @@ struct VlStore {
   __device__ static uint32_t set_front(HeapCore* h, ClassState* q, uint32_t cur) {
     uint32_t ret = 0;
     for (uint32_t i = 0; i < (1u << 16); ++i) {
-      uint32_t nx = ld_acquire(&h->meta[cur].next);
+      uint32_t nx = next_of(h, cur);
       if (nx == kEmpty) break;
       if (atomicCAS(&q->front_ptr, cur, nx) != cur) break;
       ++ret;
@@ -331,9 +397,11 @@ struct VlStore {
     uint32_t old = ld_relaxed(&q->old_ptr);
     for (uint32_t guard = 0; freed > 0 && guard < (1u << 20); ++guard) {
       uint32_t nx = ld_acquire(&h->meta[old].next);
+      if (nx >= kInstalling) break;
       uint32_t seen = atomicCAS(&q->old_ptr, old, nx);
       if (seen == old) {
         --freed;
+        if (q->clean_on_recycle) clean_queue_chunk(h, old);
         reuse_put(h, &h->reuse[0], old);
         old = nx;
       } else {
@@ -361,98 +429,140 @@ struct VlStore {
     if (old - sub == kQcSpots) on_empty(h, q, c);
   }
 
-  // A producer at the start of a queue chunk links the next one (QueueChunk_impl.cuh:144-158).
+  // A producer at the start of a queue chunk links the next one
+  // (QueueChunk_impl.cuh:144-158).  A link needs its predecessor, so linking
+  // is a chain; when producers already hold positions several queue chunks
+  // ahead (a burst), the chain is built up to 8 chunks at a time and offered
+  // in one CAS.  A lone producer is never further than one chunk ahead, so it
+  // links exactly one chunk, as the reference does.
   __device__ static void preallocate(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos) {
-    uint32_t nq = new_queue_chunk(h, q->inst, pos + kQcSpots);
-    if (nq != kEmpty) st_release(&h->meta[c].next, nq);
+    uint32_t* link = &h->meta[c].next;
+    if (ld_relaxed(link) != kEmpty) return;
+    const uint32_t back = ld_relaxed(&q->back.v);
+    uint32_t ahead = static_cast<int32_t>(back - pos) > static_cast<int32_t>(2u * kQcSpots)
+                         ? (back - pos) / kQcSpots - 1u : 1u;
+    if (ahead > 8u) ahead = 8u;
+    const uint32_t first = new_queue_chunk(h, q->inst, pos + kQcSpots);
+    if (first == kEmpty) return;
+    uint32_t last = first;
+    for (uint32_t i = 1; i < ahead; ++i) {
+      uint32_t nq = new_queue_chunk(h, q->inst, pos + (i + 1u) * kQcSpots);
+      if (nq == kEmpty) break;
+      st_relaxed(&h->meta[last].next, nq);
+      last = nq;
+    }
+    __threadfence();
+    if (atomicCAS(link, kEmpty, first) == kEmpty) {
+      for (uint32_t cc = first, i = 0; i < 8u; ++i) {
+        remember(h, q, cc, pos + (i + 1u) * kQcSpots);
+        if (cc == last) break;
+        cc = ld_relaxed(&h->meta[cc].next);
+      }
+    } else {
+      for (uint32_t cc = first, i = 0; i < 8u; ++i) {
+        uint32_t nx = ld_relaxed(&h->meta[cc].next);
+        reuse_put(h, &h->reuse[0], cc);
+        if (cc == last) break;
+        cc = nx;
+      }
+    }
+  }
+
+  __device__ static Group half_of(const Group& g, uint32_t pos, uint32_t first) {
+    const bool second = pos / kQcSpots != first / kQcSpots;
+    const uint32_t m2 = __ballot_sync(g.mask, second);
+    return make_group(second ? m2 : (g.mask & ~m2));
   }
 
   template <bool PageQueue, typename Value>
   __device__ static void publish_range(HeapCore* h, ClassState* q, const Group& g, uint32_t b, uint32_t E,
                                        uint32_t chunk, uint32_t entries_per_chunk, Value&& value) {
     const uint32_t n = static_cast<uint32_t>(g.size);
-    const uint32_t rounds = (E + n - 1u) / n;
     uint32_t c1 = kEmpty;
-    if (g.is_leader()) c1 = locate(h, ld_acquire(&q->back_ptr), b);
+    if (g.is_leader()) c1 = locate_live(h, q, ld_acquire(&q->back_ptr), b);
     c1 = bcast(g, c1);
-    if (c1 == kEmpty || c1 == kBehind) { set_status(h, kErrCorrupt); return; }
-    const uint32_t split = kQcSpots - (b % kQcSpots);
-    // the lane holding the first position of a queue chunk links the next one
-    for (uint32_t i = 0; i < rounds; ++i) {
-      uint32_t j = static_cast<uint32_t>(g.rank) + i * n;
-      if (j < E && ((b + j) % kQcSpots) == 0u) preallocate(h, q, j < split ? c1 : next_of(h, c1), b + j);
+    if (c1 == kEmpty || c1 == kBehind) {
+      if (g.is_leader()) set_status(h, kErrCorrupt);
+      return;
     }
-    uint32_t c2 = E > split ? kEmpty : c1;
-    for (uint32_t i = 0; i < rounds; ++i) {
-      uint32_t j = static_cast<uint32_t>(g.rank) + i * n;
-      int src = j < E ? lane_of_rank(g.mask, static_cast<int>(j / entries_per_chunk)) : g.leader;
-      uint32_t cj = __shfl_sync(g.mask, chunk, src);
-      if (j < E) {
-        uint32_t qc = c1;
-        if (j >= split) {
-          if (c2 == kEmpty) c2 = next_of(h, c1);
-          qc = c2;
+    const uint32_t room = kQcSpots - (b % kQcSpots);
+    const uint32_t split = E < room ? E : room;
+    if (b % kQcSpots == 0u && g.is_leader()) preallocate(h, q, c1, b);
+    for (uint32_t half = 0; half < 2u; ++half) {
+      const uint32_t j0 = half ? split : 0u, j1 = half ? E : split;
+      if (j0 >= j1) continue;
+      uint32_t qc = c1;
+      if (half) {
+        if (g.is_leader()) {
+          qc = next_of(h, c1);
+          if (qc != kEmpty) preallocate(h, q, qc, b + j0);   // b + split starts a queue chunk
         }
+        qc = bcast(g, qc);
         if (qc == kEmpty) continue;
-        uint32_t* s = queue_slots(h, qc) + ((b + j) % kQcSpots);
-        st_relaxed(s, value(j, cj));   // linked slots are written once per lap (enqueueLinked)
       }
-    }
-    __syncwarp(g.mask);
-    __threadfence();
-    if (g.is_leader()) {
-      uint32_t m1 = E < split ? E : split;
-      count_enqueued(h, q, c1, m1);
-      if (E > m1) {
-        uint32_t cc = next_of(h, c1);
-        if (cc != kEmpty) count_enqueued(h, q, cc, E - m1);
+      const uint32_t r2 = (j1 - j0 + n - 1u) / n;
+      for (uint32_t i = 0; i < r2; ++i) {
+        uint32_t j = j0 + static_cast<uint32_t>(g.rank) + i * n;
+        int src = j < j1 ? lane_of_rank(g.mask, static_cast<int>(j / entries_per_chunk)) : g.leader;
+        uint32_t cj = __shfl_sync(g.mask, chunk, src);
+        if (j < j1) st_relaxed(queue_slots(h, qc) + ((b + j) % kQcSpots), value(j, cj));   // enqueueLinked
       }
+      __syncwarp(g.mask);
+      __threadfence();
+      if (g.is_leader()) count_enqueued(h, q, qc, j1 - j0);
     }
   }
 
   __device__ static void publish_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos, uint32_t v) {
-    uint32_t first = bcast(g, pos);
+    const uint32_t first = bcast(g, pos);
     uint32_t c1 = kEmpty;
-    if (g.is_leader()) c1 = locate(h, ld_acquire(&q->back_ptr), first);
+    if (g.is_leader()) c1 = locate_live(h, q, ld_acquire(&q->back_ptr), first);
     c1 = bcast(g, c1);
-    uint32_t qc = kEmpty;
-    if (c1 != kEmpty && c1 != kBehind) {
-      qc = (pos / kQcSpots == first / kQcSpots) ? c1 : next_of(h, c1);
-      if (qc != kEmpty) {
-        if (pos % kQcSpots == 0u) preallocate(h, q, qc, pos);
-        st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), v);
-      }
-    } else {
-      set_status(h, kErrCorrupt);
+    const Group sg = half_of(g, pos, first);
+    if (c1 == kEmpty || c1 == kBehind) {
+      if (g.is_leader()) set_status(h, kErrCorrupt);
+      return;
     }
-    __syncwarp(g.mask);
+    uint32_t qc = c1;
+    if (pos / kQcSpots != first / kQcSpots) {
+      if (sg.is_leader()) qc = next_of(h, c1);
+      qc = bcast(sg, qc);
+    }
+    if (qc != kEmpty) {
+      if (pos % kQcSpots == 0u) preallocate(h, q, qc, pos);
+      st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), v);
+    }
+    __syncwarp(sg.mask);
     __threadfence();
-    Group cg = group_by(g.mask, qc);
-    if (cg.is_leader() && qc != kEmpty) count_enqueued(h, q, qc, static_cast<uint32_t>(cg.size));
+    if (sg.is_leader() && qc != kEmpty) count_enqueued(h, q, qc, static_cast<uint32_t>(sg.size));
   }
 
   __device__ static uint32_t consume_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos) {
-    uint32_t first = bcast(g, pos);
+    const uint32_t first = bcast(g, pos);
     uint32_t c1 = kEmpty;
-    if (g.is_leader()) c1 = locate(h, ld_acquire(&q->front_ptr), first);
+    if (g.is_leader()) c1 = locate_live(h, q, ld_acquire(&q->front_ptr), first);
     c1 = bcast(g, c1);
-    uint32_t qc = kEmpty, v = kEmpty;
-    if (c1 != kEmpty && c1 != kBehind) {
-      qc = (pos / kQcSpots == first / kQcSpots) ? c1 : next_of(h, c1);
-      if (qc != kEmpty) v = take_slot(h, queue_slots(h, qc) + (pos % kQcSpots));
-    } else {
-      set_status(h, kErrCorrupt);
+    const Group sg = half_of(g, pos, first);
+    if (c1 == kEmpty || c1 == kBehind) {
+      if (g.is_leader()) set_status(h, kErrCorrupt);
+      return kEmpty;
     }
-    __syncwarp(g.mask);
-    Group cg = group_by(g.mask, qc);
-    if (cg.is_leader() && qc != kEmpty) count_removed(h, q, qc, static_cast<uint32_t>(cg.size));
+    uint32_t qc = c1;
+    if (pos / kQcSpots != first / kQcSpots) {
+      if (sg.is_leader()) qc = next_of(h, c1);
+      qc = bcast(sg, qc);
+    }
+    uint32_t v = kEmpty;
+    if (qc != kEmpty) v = take_slot(h, queue_slots(h, qc) + (pos % kQcSpots));
+    __syncwarp(sg.mask);
+    if (sg.is_leader() && qc != kEmpty) count_removed(h, q, qc, static_cast<uint32_t>(sg.size));
     return v;
   }
 
   // ---- chunk-queue side
   __device__ static bool enqueue_one(HeapCore* h, ClassState* q, uint32_t c, uint32_t* qpos) {
     uint32_t b = atomicAdd(&q->back.v, 1u);
-    uint32_t qc = locate(h, ld_acquire(&q->back_ptr), b);
+    uint32_t qc = locate_live(h, q, ld_acquire(&q->back_ptr), b);
     if (qc == kEmpty || qc == kBehind) { set_status(h, kErrCorrupt); return false; }
     if (b % kQcSpots == 0u) preallocate(h, q, qc, b);
     st_relaxed(qpos, b);
@@ -475,29 +585,41 @@ struct VlStore {
     return ld_acquire(queue_slots(h, qc) + (pos % kQcSpots));
   }
   __device__ static void remove(HeapCore* h, ClassState* q, uint32_t pos) {
-    uint32_t qc = locate(h, ld_acquire(&q->front_ptr), pos);
+    uint32_t qc = locate_live(h, q, ld_acquire(&q->front_ptr), pos);
     if (qc == kEmpty || qc == kBehind) return;
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
     __threadfence();
     count_removed(h, q, qc, 1u);
   }
   __device__ static void advance_front(HeapCore* h, ClassState* q) {
-    uint32_t cur = ld_acquire(&q->front_ptr);
-    for (uint32_t i = 0; i < 64u; ++i) {
-      uint32_t f = ld_relaxed(&q->front.v);
-      if (static_cast<int32_t>(ld_relaxed(&q->back.v) - f) <= 0) return;
-      uint32_t qc = locate(h, cur, f);
-      if (qc == kEmpty) return;
-      if (qc == kBehind) {
-        // front lags the first live queue chunk: everything before it is gone
-        uint32_t start = ld_relaxed(&h->meta[cur].vstart);
-        start -= start % kQcSpots;
-        if (static_cast<int32_t>(start - f) > 0) atomicCAS(&q->front.v, f, start);
-        continue;
+    const uint32_t f = ld_relaxed(&q->front.v);
+    const uint32_t back = ld_relaxed(&q->back.v);
+    if (static_cast<int32_t>(back - f) <= 0) return;
+    const uint32_t first = ld_acquire(&q->front_ptr);
+    uint32_t qc = locate(h, first, f);
+    if (qc == kEmpty) return;
+    uint32_t g = f;
+    if (qc == kBehind) {
+      // front lags the first live queue chunk: everything before it is gone
+      const uint32_t vs = ld_relaxed(&h->meta[first].vstart);
+      g = vs - vs % kQcSpots;
+      qc = first;
+    }
+    while (g != back && g - f < 4096u) {
+      if (g % kQcSpots == 0u && g != f) {
+        const uint32_t nx = ld_acquire(&h->meta[qc].next);
+        if (nx >= kInstalling) break;
+        qc = nx;
       }
-      cur = qc;
-      if (ld_acquire(queue_slots(h, qc) + (f % kQcSpots)) != kTomb) return;
-      atomicCAS(&q->front.v, f, f + 1u);
+      if (ld_acquire(queue_slots(h, qc) + (g % kQcSpots)) != kTomb) break;
+      ++g;
+    }
+    if (static_cast<int32_t>(g - f) <= 0) return;
+    uint32_t cur = f;
+    for (;;) {
+      const uint32_t seen = atomicCAS(&q->front.v, cur, g);
+      if (seen == cur || static_cast<int32_t>(seen - g) >= 0) return;
+      cur = seen;
     }
   }
 };
