@@ -151,6 +151,11 @@ int ouro_check_heap(ouro_heap* h, ouro_heap_report* out);
  * in G operations per second. */
 int ouro_measure_atomics(int mode, double* gops);
 
+/* Diagnostic counters of the chunk-queue scan: groups, probes, misses, jumps,
+ * restarts, -, tomb helps, -.  All zero unless the library was built with
+ * -DOURO_SCAN_STATS.  No counterpart in the reference. */
+int ouro_scan_stats(ouro_heap* h, uint64_t* out8, int clear);
+
 const char* ouro_status_string(int code);
 
 #ifdef __cplusplus

@@ -37,7 +37,8 @@ FLAG_OOM, FLAG_TIMEOUT, FLAG_CORRUPT, FLAG_QUEUE_FULL = 1, 2, 4, 8
 EXPORTS = (
     "ouro_create", "ouro_destroy", "ouro_device_handle", "ouro_get_info", "ouro_alloc", "ouro_free",
     "ouro_trace", "ouro_state", "ouro_get_status", "ouro_write_pattern", "ouro_verify_pattern",
-    "ouro_check_allocations", "ouro_check_heap", "ouro_measure_atomics", "ouro_status_string",
+    "ouro_check_allocations", "ouro_check_heap", "ouro_measure_atomics", "ouro_scan_stats",
+    "ouro_status_string",
 )
 
 
@@ -91,6 +92,7 @@ def lib():
         L.ouro_check_allocations.argtypes = [p, p, u32, u32, p, ctypes.POINTER(_AllocReport)]
         L.ouro_check_heap.argtypes = [p, ctypes.POINTER(_HeapReport)]
         L.ouro_measure_atomics.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
+        L.ouro_scan_stats.argtypes = [p, p, i]
         L.ouro_status_string.argtypes = [i]
         L.ouro_status_string.restype = ctypes.c_char_p
         _lib = L
@@ -203,6 +205,12 @@ class Ouroboros:
         _check(lib().ouro_check_allocations(self._handle(), _addr(ptrs), n, size, _addr(sizes), ctypes.byref(out)),
                "ouro_check_allocations")
         return {k: int(getattr(out, k)) for k, _ in _AllocReport._fields_}
+
+    def scan_stats(self, clear: bool = False) -> dict:
+        out = np.zeros(8, dtype=np.uint64)
+        _check(lib().ouro_scan_stats(self._handle(), out.ctypes.data, int(clear)), "ouro_scan_stats")
+        names = ("groups", "probes", "misses", "runs", "unused4", "unused5", "unused6", "unused7")
+        return {k: int(x) for k, x in zip(names, out)}
 
     def check_heap(self) -> dict:
         out = _HeapReport()

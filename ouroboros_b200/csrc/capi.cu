@@ -569,6 +569,18 @@ int ouro_check_heap(ouro_heap* h, ouro_heap_report* out) {
 }
 
 
+// Diagnostic counters of the chunk-queue scan (zero unless the library was
+// built with OURO_SCAN_STATS); no counterpart in the reference.
+int ouro_scan_stats(ouro_heap* h, uint64_t* out8, int clear) {
+  if (!h || !out8) return OURO_ERR_ARG;
+  if (cudaDeviceSynchronize() != cudaSuccess) return OURO_ERR_CUDA;
+  Line<unsigned long long> v[8];
+  if (cudaMemcpy(v, h->dev->scan, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
+  for (int i = 0; i < 8; ++i) out8[i] = v[i].v;
+  if (clear && cudaMemset(h->dev->scan, 0, sizeof(v)) != cudaSuccess) return OURO_ERR_CUDA;
+  return OURO_OK;
+}
+
 int ouro_measure_atomics(int mode, double* gops) {
   if (!gops || mode < 0 || mode > 2) return OURO_ERR_ARG;
   int sms = 0;

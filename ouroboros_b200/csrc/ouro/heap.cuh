@@ -36,6 +36,8 @@ struct alignas(128) ClassState {
   Line<uint32_t> front;           // consumer position (virtual)
   Line<uint32_t> back;            // producer position (virtual)
   Line<int32_t> entries;          // chunk-based: entries in the queue (count_)
+  Line<uint32_t> cursor;          // chunk-based: next-fit scan cursor for contended groups
+  Line<uint32_t> advancing;       // chunk-based: try-lock of the lane moving the front
   // cold line
   uint32_t* ring;                 // standard: the ring; virtualized array: the index array
   uint32_t ring_mask;
@@ -73,6 +75,9 @@ struct alignas(128) HeapCore {
   Line<unsigned long long> chunk_allocs;
   ReuseQueue reuse[2];
   ClassState cls[kNumClasses];
+  // chunk-queue scan counters, only written when built with OURO_SCAN_STATS:
+  // groups, probes, misses, jumps, restarts at the back, claim retries, tomb helps
+  Line<unsigned long long> scan[8];
 };
 
 constexpr size_t kCoreBytes = 16384;

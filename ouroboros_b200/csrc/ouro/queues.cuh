@@ -153,6 +153,17 @@ __device__ void ensure_enqueued(HeapCore* h, ClassState* q, uint32_t c) {
   if (atomicCAS(&h->meta[c].queue_pos, kEmpty, kPending) == kEmpty) chunk_enqueue<Store>(h, q, c);
 }
 
+// The front moves over removed entries; one lane at a time does it (a
+// try-lock nobody waits on), so removals all over the queue do not turn into
+// thousands of lanes scanning the same run.
+template <class Store>
+__device__ void help_front(HeapCore* h, ClassState* q) {
+  if (atomicCAS(&q->advancing.v, 0u, 1u) != 0u) return;
+  Store::advance_front(h, q);
+  __threadfence();
+  atomicExch(&q->advancing.v, 0u);
+}
+
 // Remove the entry of an exhausted chunk (the DEQUEUE_CHUNK mode of
 // ChunkQueue_impl.cuh:128-137) and advance the front over removed entries.
 template <class Store>
@@ -166,7 +177,7 @@ __device__ void chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32_t p
   if (atomicCAS(qp, pos, kEmpty) != pos) return;   // someone else removed or moved it
   Store::remove(h, q, pos);
   atomicSub(&q->entries.v, 1);
-  Store::advance_front(h, q);
+  help_front<Store>(h, q);
   __threadfence();
   if (ld_relaxed(&h->meta[c].count) > 0) ensure_enqueued<Store>(h, q, c);
 }
@@ -267,6 +278,24 @@ __device__ uint32_t chunk_grow(HeapCore* h, ClassState* q, const Group& g, uint3
   return got;
 }
 
+// Next-fit run for a contended group: `run` consecutive queue positions from
+// the class's scan cursor, mapped into the current window [front, back).
+template <class Store>
+__device__ uint32_t claim_run(HeapCore* h, ClassState* q, uint32_t run) {
+  const uint32_t c = atomicAdd(&q->cursor.v, run);
+  const uint32_t f = ld_relaxed(&q->front.v);
+  const uint32_t w = ld_relaxed(&q->back.v) - f;
+  if (static_cast<int32_t>(w) <= 0) return f;
+  return f + (c - f) % w;
+}
+
+// ChunkQueue_impl.cuh:82-148 allocPage, for a group.  The first probe is the
+// front entry, which is where the reference starts and where a lone lane
+// always finds pages (exhausted chunks leave the queue at once).  A group that
+// misses there is contending with others and continues with next-fit runs of
+// ceil(need / pages-per-chunk) entries taken from the scan cursor, so
+// concurrent groups work on disjoint chunks instead of all scanning from the
+// front.
 template <class Store>
 __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
   uint32_t granted = sem_acquire(h, q, g, [&](uint32_t k) { return chunk_grow<Store>(h, q, g, k); });
@@ -280,15 +309,20 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
   Group s = make_group(smask);
   bool served = false;
   uint32_t page = 0, chunk = kEmpty;
-  uint32_t pos = 0;
+  uint32_t pos = 0, run_end = 0;
   typename Store::Cursor cur{};
   if (s.is_leader()) {
     pos = ld_relaxed(&q->front.v);
+    run_end = pos + 1u;
     cur = Store::cursor(q);
   }
   uint32_t need = static_cast<uint32_t>(s.size);
-  uint32_t it = 0, misses = 0, tombs = 0;
-  uint32_t rng = (blockIdx.x * 32u + threadIdx.x / 32u) * 2654435761u + 12345u;
+#ifdef OURO_SCAN_STATS
+  unsigned long long st_probe = 0, st_miss = 0, st_run = 0;
+#define OURO_STAT(x) ++(x)
+#else
+#define OURO_STAT(x) ((void)0)
+#endif
   for (uint32_t iter = 0;; ++iter) {
     uint32_t c = kEmpty, got = 0, last = 0;
     if (s.is_leader()) {
@@ -296,16 +330,16 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
         note_timeout(h);
         c = kTomb;
       } else {
-        uint32_t v = Store::peek(h, q, pos, cur);
-        if (v == kTomb && ++tombs >= 4u) {
-          // removed entries ahead of us: help the front past them and skip
-          tombs = 0;
-          Store::advance_front(h, q);
-          const uint32_t f = ld_relaxed(&q->front.v);
-          if (static_cast<int32_t>(f - pos) > 0) pos = f;
+        if (pos == run_end) {
+          const uint32_t run = (need + q->ppc - 1u) / q->ppc;
+          pos = claim_run<Store>(h, q, run);
+          run_end = pos + run;
+          OURO_STAT(st_run);
         }
+        const uint32_t v = Store::peek(h, q, pos, cur);
+        OURO_STAT(st_probe);
+        if (v == kTomb && iter == 0u) help_front<Store>(h, q);   // the front entry is gone
         const bool live = v < kTomb && v < h->max_chunks && ld_relaxed(&h->meta[v].page_size) == q->page_size;
-        if (live && ld_relaxed(&h->meta[v].count) <= 0) ++misses;
         if (live && ld_relaxed(&h->meta[v].count) > 0) {
           int32_t old = atomicSub(&h->meta[v].count, static_cast<int32_t>(need));
           got = old <= 0 ? 0u : (static_cast<uint32_t>(old) < need ? static_cast<uint32_t>(old) : need);
@@ -318,25 +352,9 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
           c = got ? v : kEmpty;
         }
         if (!got) {
-          if (live) ++misses;
-          // nothing here: next position; at the back, start over from the front
+          OURO_STAT(st_miss);
           ++pos;
-          const uint32_t back = ld_relaxed(&q->back.v);
-          if (static_cast<int32_t>(back - pos) <= 0) {
-            pos = ld_relaxed(&q->front.v);
-            cur = Store::cursor(q);
-            backoff(it);
-          } else if (misses >= 2u) {
-            // Many groups scan from the same front; after two exhausted
-            // chunks jump to a random position of the remaining window.  A
-            // lone lane never misses (exhausted chunks leave the queue at
-            // once), so it keeps the reference's front-first order.
-            misses = 0;
-            rng = rng * 1664525u + 1013904223u;
-            uint32_t front = ld_relaxed(&q->front.v);
-            if (static_cast<int32_t>(pos - front) < 0) pos = front;
-            pos += (rng >> 8) % (back - pos);
-          }
+          if (static_cast<int32_t>(ld_relaxed(&q->back.v) - pos) <= 0) run_end = pos;   // next: a fresh run
         }
       }
     }
@@ -355,8 +373,19 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
       }
       need = static_cast<uint32_t>(__popc(__ballot_sync(s.mask, !served)));
       if (need == 0u) break;
+    } else if (s.is_leader() && iter == 0u) {
+      run_end = pos;   // missed at the front: contended, switch to next-fit runs
     }
   }
+#ifdef OURO_SCAN_STATS
+  if (s.is_leader()) {
+    atomicAdd(&h->scan[0].v, 1ull);
+    atomicAdd(&h->scan[1].v, st_probe);
+    atomicAdd(&h->scan[2].v, st_miss);
+    atomicAdd(&h->scan[3].v, st_run);
+  }
+#endif
+#undef OURO_STAT
   return page_address(h, chunk, page, q->page_shift);
 }
 
@@ -388,7 +417,7 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
           if (qp != kPending && qp != kEmpty && atomicCAS(&m->queue_pos, qp, kEmpty) == qp) {
             Store::remove(h, q, qp);
             atomicSub(&q->entries.v, 1);
-            Store::advance_front(h, q);
+            help_front<Store>(h, q);
           }
           reuse_put(h, &h->reuse[q->inst], c);
           flashed = 1u;

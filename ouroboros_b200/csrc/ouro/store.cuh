@@ -99,7 +99,7 @@ struct FlatStore {
     const uint32_t f = ld_relaxed(&q->front.v);
     const uint32_t back = ld_relaxed(&q->back.v);
     uint32_t g = f;
-    while (g != back && g - f < 4096u && ld_relaxed(slot(q, g)) == kTomb) ++g;
+    while (g != back && g - f < 8192u && ld_relaxed(slot(q, g)) == kTomb) ++g;
     if (g == f) return;
     uint32_t cur = f;
     for (;;) {
@@ -263,7 +263,7 @@ struct VaStore {
     const uint32_t f = ld_relaxed(&q->front.v);
     const uint32_t back = ld_relaxed(&q->back.v);
     uint32_t g = f, qc = kEmpty;
-    while (g != back && g - f < 4096u) {
+    while (g != back && g - f < 8192u) {
       if (g == f || g % kQcSpots == 0u) {
         qc = ld_acquire(q->ring + vid(g));
         if (qc >= kInstalling || ld_relaxed(&h->meta[qc].vstart) / kQcSpots != g / kQcSpots) break;
@@ -575,7 +575,8 @@ struct VlStore {
   struct Cursor { uint32_t chunk; };
   __device__ static Cursor cursor(ClassState* q) { return Cursor{ld_acquire(&q->front_ptr)}; }
   __device__ static uint32_t peek(HeapCore* h, ClassState* q, uint32_t pos, Cursor& cur) {
-    uint32_t qc = locate(h, cur.chunk, pos);
+    uint32_t qc = recall(h, q, pos);
+    if (qc == kEmpty) qc = locate(h, cur.chunk, pos);
     if (qc == kBehind) {
       cur.chunk = ld_acquire(&q->front_ptr);
       return kTomb;
@@ -605,11 +606,13 @@ struct VlStore {
       g = vs - vs % kQcSpots;
       qc = first;
     }
-    while (g != back && g - f < 4096u) {
-      if (g % kQcSpots == 0u && g != f) {
+    uint32_t range = g / kQcSpots;   // virtual queue chunk that qc holds
+    while (g != back && g - f < 8192u) {
+      if (g / kQcSpots != range) {
         const uint32_t nx = ld_acquire(&h->meta[qc].next);
         if (nx >= kInstalling) break;
         qc = nx;
+        range = g / kQcSpots;
       }
       if (ld_acquire(queue_slots(h, qc) + (g % kQcSpots)) != kTomb) break;
       ++g;
