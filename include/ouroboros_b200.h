@@ -151,10 +151,13 @@ int ouro_check_heap(ouro_heap* h, ouro_heap_report* out);
  * in G operations per second. */
 int ouro_measure_atomics(int mode, double* gops);
 
-/* Diagnostic counters of the chunk-queue scan: groups, probes, misses, jumps,
- * restarts, -, tomb helps, -.  All zero unless the library was built with
- * -DOURO_SCAN_STATS.  No counterpart in the reference. */
-int ouro_scan_stats(ouro_heap* h, uint64_t* out8, int clear);
+/* Diagnostic counters of the chunk-based allocation path, 12 words: groups,
+ * probes, misses, next-fit runs; SM cycles summed over group leaders spent in
+ * the semaphore, the scan, dequeues and page claims; groups slower than 2^20
+ * cycles; the slowest group's cycles; front advances and the cycles inside
+ * them.  All zero unless the library was built with -DOURO_SCAN_STATS.  No
+ * counterpart in the reference. */
+int ouro_scan_stats(ouro_heap* h, uint64_t* out12, int clear);
 
 const char* ouro_status_string(int code);
 

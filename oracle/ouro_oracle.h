@@ -8,11 +8,11 @@
  * and the CPU-baseline leg of bench.py may load it.  Nothing in the product
  * path calls it.
  *
- * Pinning: the layout arithmetic is checked against tests/golden/layout.json
- * (a host probe compiled against the reference headers) and every trace result
- * against tests/golden/trace_*.npz (the reference's own sm_100a build running
- * the same trace with one GPU thread).  Both generators live beside the
- * fixtures.
+ * Pinning: the layout arithmetic (maxChunks, allocation size) and every trace
+ * result and counter are checked against tests/golden/trace_*.npz: the
+ * reference's own sm_100a build running the same traces with one GPU thread on
+ * a 1 GiB heap (generator: tests/golden/make_golden.py), plus the reference's
+ * maxChunks at 1..32 GiB from a host probe of its types.
  *
  * Result encoding (shared with the CUDA allocator's trace entry point):
  *   bits  0..31  MemoryIndex = chunk << 9 | page        (MemoryIndex.cuh:6-51)

@@ -207,9 +207,10 @@ class Ouroboros:
         return {k: int(getattr(out, k)) for k, _ in _AllocReport._fields_}
 
     def scan_stats(self, clear: bool = False) -> dict:
-        out = np.zeros(8, dtype=np.uint64)
+        out = np.zeros(12, dtype=np.uint64)
         _check(lib().ouro_scan_stats(self._handle(), out.ctypes.data, int(clear)), "ouro_scan_stats")
-        names = ("groups", "probes", "misses", "runs", "unused4", "unused5", "unused6", "unused7")
+        names = ("groups", "probes", "misses", "runs", "cyc_sem", "cyc_scan", "cyc_dequeue", "cyc_claim",
+                 "slow_groups", "cyc_max", "front_advances", "cyc_front")
         return {k: int(x) for k, x in zip(names, out)}
 
     def check_heap(self) -> dict:

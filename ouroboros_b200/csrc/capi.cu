@@ -569,14 +569,14 @@ int ouro_check_heap(ouro_heap* h, ouro_heap_report* out) {
 }
 
 
-// Diagnostic counters of the chunk-queue scan (zero unless the library was
-// built with OURO_SCAN_STATS); no counterpart in the reference.
-int ouro_scan_stats(ouro_heap* h, uint64_t* out8, int clear) {
-  if (!h || !out8) return OURO_ERR_ARG;
+// Diagnostic counters of the chunk-based allocation path (zero unless the
+// library was built with OURO_SCAN_STATS); no counterpart in the reference.
+int ouro_scan_stats(ouro_heap* h, uint64_t* out, int clear) {
+  if (!h || !out) return OURO_ERR_ARG;
   if (cudaDeviceSynchronize() != cudaSuccess) return OURO_ERR_CUDA;
-  Line<unsigned long long> v[8];
+  Line<unsigned long long> v[kScanCounters];
   if (cudaMemcpy(v, h->dev->scan, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
-  for (int i = 0; i < 8; ++i) out8[i] = v[i].v;
+  for (uint32_t i = 0; i < kScanCounters; ++i) out[i] = v[i].v;
   if (clear && cudaMemset(h->dev->scan, 0, sizeof(v)) != cudaSuccess) return OURO_ERR_CUDA;
   return OURO_OK;
 }

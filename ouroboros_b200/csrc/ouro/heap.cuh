@@ -56,6 +56,8 @@ struct alignas(128) ReuseQueue {
   uint32_t* ring;
 };
 
+constexpr uint32_t kScanCounters = 12u;
+
 // Device-resident control block, the object device code calls malloc/free on.
 struct alignas(128) HeapCore {
   // cold configuration line
@@ -75,9 +77,11 @@ struct alignas(128) HeapCore {
   Line<unsigned long long> chunk_allocs;
   ReuseQueue reuse[2];
   ClassState cls[kNumClasses];
-  // chunk-queue scan counters, only written when built with OURO_SCAN_STATS:
-  // groups, probes, misses, jumps, restarts at the back, claim retries, tomb helps
-  Line<unsigned long long> scan[8];
+  // chunk-based path counters, only written when built with OURO_SCAN_STATS:
+  // groups, probes, misses, next-fit runs; leader cycles in semaphore, scan,
+  // dequeue, claim; groups slower than 2^20 cycles, slowest group's cycles,
+  // front advances, cycles inside front advances
+  Line<unsigned long long> scan[kScanCounters];
 };
 
 constexpr size_t kCoreBytes = 16384;

@@ -159,9 +159,16 @@ __device__ void ensure_enqueued(HeapCore* h, ClassState* q, uint32_t c) {
 template <class Store>
 __device__ void help_front(HeapCore* h, ClassState* q) {
   if (atomicCAS(&q->advancing.v, 0u, 1u) != 0u) return;
+#ifdef OURO_SCAN_STATS
+  const long long t0 = clock64();
+#endif
   Store::advance_front(h, q);
   __threadfence();
   atomicExch(&q->advancing.v, 0u);
+#ifdef OURO_SCAN_STATS
+  atomicAdd(&h->scan[10].v, 1ull);
+  atomicAdd(&h->scan[11].v, static_cast<unsigned long long>(clock64() - t0));
+#endif
 }
 
 // Remove the entry of an exhausted chunk (the DEQUEUE_CHUNK mode of
@@ -298,7 +305,13 @@ __device__ uint32_t claim_run(HeapCore* h, ClassState* q, uint32_t run) {
 // front.
 template <class Store>
 __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
+#ifdef OURO_SCAN_STATS
+  long long t_begin = clock64(), t_claim = 0, t_deq = 0;
+#endif
   uint32_t granted = sem_acquire(h, q, g, [&](uint32_t k) { return chunk_grow<Store>(h, q, g, k); });
+#ifdef OURO_SCAN_STATS
+  const long long t_sem = clock64() - t_begin;
+#endif
   const bool in = static_cast<uint32_t>(g.rank) < granted;
   if (granted < static_cast<uint32_t>(g.size) && g.is_leader()) {
     atomicAdd(&h->oom.v, static_cast<unsigned long long>(g.size - granted));
@@ -364,13 +377,23 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
     if (got) {
       last = bcast(s, last);
       bool before = served;
+#ifdef OURO_SCAN_STATS
+      long long t0 = clock64();
+#endif
       if (q->inst == 0u) claim_pages<16u>(h, s, c, got, served, page);
       else claim_pages<1u>(h, s, c, got, served, page);
+#ifdef OURO_SCAN_STATS
+      t_claim += clock64() - t0;
+      t0 = clock64();
+#endif
       if (served && !before) chunk = c;
       if (s.is_leader()) {
         if (last) chunk_dequeue<Store>(h, q, c, pos);
         ++pos;
       }
+#ifdef OURO_SCAN_STATS
+      t_deq += clock64() - t0;
+#endif
       need = static_cast<uint32_t>(__popc(__ballot_sync(s.mask, !served)));
       if (need == 0u) break;
     } else if (s.is_leader() && iter == 0u) {
@@ -383,6 +406,13 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
     atomicAdd(&h->scan[1].v, st_probe);
     atomicAdd(&h->scan[2].v, st_miss);
     atomicAdd(&h->scan[3].v, st_run);
+    atomicAdd(&h->scan[4].v, static_cast<unsigned long long>(t_sem));
+    atomicAdd(&h->scan[5].v, static_cast<unsigned long long>(clock64() - t_begin - t_sem - t_claim - t_deq));
+    atomicAdd(&h->scan[6].v, static_cast<unsigned long long>(t_deq));
+    atomicAdd(&h->scan[7].v, static_cast<unsigned long long>(t_claim));
+    const unsigned long long total = static_cast<unsigned long long>(clock64() - t_begin);
+    if (total > (1ull << 20)) atomicAdd(&h->scan[8].v, 1ull);
+    atomicMax(&h->scan[9].v, total);
   }
 #endif
 #undef OURO_STAT

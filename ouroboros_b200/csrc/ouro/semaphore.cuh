@@ -113,7 +113,12 @@ __device__ inline uint32_t sem_acquire(HeapCore* h, ClassState* q, const Group& 
               mode = kTake;
               arg = m;
             } else if (avail < static_cast<long long>(n)) {
-              uint32_t k = static_cast<uint32_t>((static_cast<long long>(n) - avail + ppc - 1) / ppc);
+              // Size the growth on the count without the transient dips of
+              // other groups' fast-path attempts (they add their pages back),
+              // so that a burst does not allocate chunks for phantom demand.
+              const long long settled = (c < 0 ? 0 : c) + static_cast<long long>(e) * ppc - r;
+              const long long deficit = static_cast<long long>(n) - settled;
+              uint32_t k = deficit <= 0 ? 1u : static_cast<uint32_t>((deficit + ppc - 1) / ppc);
               if (k > n) k = n;
               nv = SemWord::make(c, e + k, r);
               mode = kAlloc;

@@ -172,11 +172,12 @@ struct VaStore {
       uint32_t j = static_cast<uint32_t>(g.rank) + i * n;
       if (j < E && ((b + j) % kQcSpots) == 0u) preallocate(h, q, b + j);
     }
-    const uint32_t room = kQcSpots - (b % kQcSpots);
-    const uint32_t split = E < room ? E : room;
-    for (uint32_t half = 0; half < 2u; ++half) {
-      const uint32_t j0 = half ? split : 0u, j1 = half ? E : split;
-      if (j0 >= j1) continue;
+    // A range may cover several queue chunks (a group that grew many chunks
+    // of a small class); each queue chunk's segment is written and counted on
+    // its own.
+    for (uint32_t j0 = 0, j1; j0 < E; j0 = j1) {
+      const uint32_t room = kQcSpots - ((b + j0) % kQcSpots);
+      j1 = E - j0 < room ? E : j0 + room;
       uint32_t qc = kEmpty;
       if (g.is_leader()) qc = qchunk(h, q, b + j0);
       qc = bcast(g, qc);
@@ -485,20 +486,20 @@ struct VlStore {
       if (g.is_leader()) set_status(h, kErrCorrupt);
       return;
     }
-    const uint32_t room = kQcSpots - (b % kQcSpots);
-    const uint32_t split = E < room ? E : room;
     if (b % kQcSpots == 0u && g.is_leader()) preallocate(h, q, c1, b);
-    for (uint32_t half = 0; half < 2u; ++half) {
-      const uint32_t j0 = half ? split : 0u, j1 = half ? E : split;
-      if (j0 >= j1) continue;
-      uint32_t qc = c1;
-      if (half) {
+    // A range may cover several queue chunks (a group that grew many chunks
+    // of a small class): walk the chain one segment per queue chunk.
+    uint32_t qc = c1;
+    for (uint32_t j0 = 0, j1; j0 < E; j0 = j1) {
+      const uint32_t room = kQcSpots - ((b + j0) % kQcSpots);
+      j1 = E - j0 < room ? E : j0 + room;
+      if (j0) {
         if (g.is_leader()) {
-          qc = next_of(h, c1);
-          if (qc != kEmpty) preallocate(h, q, qc, b + j0);   // b + split starts a queue chunk
+          qc = next_of(h, qc);
+          if (qc != kEmpty) preallocate(h, q, qc, b + j0);   // b + j0 starts a queue chunk
         }
         qc = bcast(g, qc);
-        if (qc == kEmpty) continue;
+        if (qc == kEmpty) break;
       }
       const uint32_t r2 = (j1 - j0 + n - 1u) / n;
       for (uint32_t i = 0; i < r2; ++i) {

@@ -108,3 +108,22 @@ def test_out_of_memory_virtualized(v):
             assert mc - 1 - 32 <= ok <= mc - 1 - 12, (ok, mc)
             assert bad == 0 and rep["overlaps"] == 0
         assert heap.status(clear=True)["flags"] & ~ob.FLAG_OOM == 0
+
+
+@pytest.mark.parametrize("size", [16, 32, 64])
+@pytest.mark.parametrize("v", ["VAP", "VLP"])
+def test_burst_grows_past_one_queue_chunk(v, size):
+    # 2^20 threads on a cold heap: the semaphore elects groups to grow many
+    # chunks at once (waiting groups' reservations add to the deficit), so one
+    # publish covers more than two 2048-entry queue chunks.  Every wait must
+    # end and every page must be handed out exactly once.
+    n = 1 << 20
+    with ob.Ouroboros(v, 4 * GiB) as heap:
+        ptrs = _ptrs(n)
+        for r in range(3):
+            rep, nulls, bad = _round(heap, ptrs, n, size, seed=r + 3)
+            assert nulls == 0 and bad == 0, (r, nulls, bad)
+            assert rep["overlaps"] == 0 and rep["misaligned"] == 0 and rep["out_of_heap"] == 0, rep
+            _idle(heap, v)
+        st = heap.status()
+        assert st["flags"] == 0 and st["timeouts"] == 0, st
