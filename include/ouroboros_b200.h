@@ -40,7 +40,8 @@ typedef enum {
   OURO_ERR_ARG = 1,      /* bad argument                                  */
   OURO_ERR_CUDA = 2,     /* a CUDA runtime call failed                    */
   OURO_ERR_NOMEM = 3,    /* cudaMalloc of the heap failed                 */
-  OURO_ERR_DEVICE = 4    /* the device reported an allocator error flag   */
+  OURO_ERR_DEVICE = 4,   /* the device reported an allocator error flag   */
+  OURO_ERR_TOO_LARGE = 5 /* beyond the fixed scratch of a no-alloc entry  */
 } ouro_status;
 
 /* Device-side error flags (ouro_heap_status.flags). */
@@ -127,6 +128,28 @@ typedef struct {
 } ouro_alloc_report;
 int ouro_check_allocations(ouro_heap* h, void* const* d_ptrs, uint32_t n, uint32_t size, const uint32_t* d_sizes,
                            ouro_alloc_report* out);
+
+/* The checks of ouro_check_allocations without allocating anything: no
+ * cudaMalloc, no cudaFree, no allocating library call.  For callers that
+ * cannot allocate device memory -- a serving loop that must not stall its
+ * other streams (cudaFree waits for the whole device), or a process whose
+ * allocator heap already holds nearly all of HBM, so that the checker's own
+ * bitmap allocation would fail.  No counterpart in the reference.
+ *
+ * The ownership bitmap is a fixed 8 MiB array inside this library
+ * (OURO_NOALLOC_BITMAP_BYTES; every GPU that loads the library holds it until
+ * exit).  It covers heaps of up to 1 GiB of chunk data (max_chunks <= 131072);
+ * larger heaps return OURO_ERR_TOO_LARGE.  The current device must be the
+ * heap's.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and keeps it; make that first call before any stream
+ * capture.  Each call clears the bitmap words its heap uses and *d_report
+ * (an ouro_alloc_report in DEVICE memory, filled in stream order; nothing is
+ * synchronized).  All calls share the one array: calls whose work overlaps on
+ * the GPU (other streams, or other host threads without ordering) race and
+ * give wrong counts. */
+#define OURO_NOALLOC_BITMAP_BYTES (8u << 20)
+int ouro_check_allocations_noalloc(ouro_heap* h, void* const* d_ptrs, uint32_t n, uint32_t size,
+                                   const uint32_t* d_sizes, ouro_alloc_report* d_report, void* stream);
 
 /* Heap accounting invariants at quiescence (no allocation in flight), per
  * class: pages owned by the class's chunks, free pages recorded in chunk

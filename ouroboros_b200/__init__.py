@@ -38,7 +38,7 @@ EXPORTS = (
     "ouro_create", "ouro_destroy", "ouro_device_handle", "ouro_get_info", "ouro_alloc", "ouro_free",
     "ouro_trace", "ouro_state", "ouro_get_status", "ouro_write_pattern", "ouro_verify_pattern",
     "ouro_check_allocations", "ouro_check_heap", "ouro_measure_atomics", "ouro_scan_stats",
-    "ouro_status_string",
+    "ouro_status_string", "ouro_check_allocations_noalloc",
 )
 
 
@@ -93,6 +93,7 @@ def lib():
         L.ouro_check_heap.argtypes = [p, ctypes.POINTER(_HeapReport)]
         L.ouro_measure_atomics.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
         L.ouro_scan_stats.argtypes = [p, p, i]
+        L.ouro_check_allocations_noalloc.argtypes = [p, p, u32, u32, p, p, p]
         L.ouro_status_string.argtypes = [i]
         L.ouro_status_string.restype = ctypes.c_char_p
         _lib = L

@@ -6,6 +6,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -259,6 +260,8 @@ const char* ouro_status_string(int code) {
     case OURO_ERR_CUDA: return "CUDA runtime error";
     case OURO_ERR_NOMEM: return "device out of memory";
     case OURO_ERR_DEVICE: return "allocator reported an error on the device";
+    case OURO_ERR_TOO_LARGE:
+      return "heap too large for the fixed scratch of ouro_check_allocations_noalloc (at most 1 GiB of chunk data)";
     default: return "unknown status";
   }
 }
@@ -612,6 +615,73 @@ int ouro_measure_atomics(int mode, double* gops) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(a);
+  return cuda_rc(e);
+}
+
+// ------------------------------------------------ allocation-free checker
+//
+// ouro_check_allocations takes its ownership bitmap (one bit per 16 bytes of
+// the heap) from cudaMalloc and gives it back with cudaFree.  Some callers
+// cannot do either: a serving loop that must not stall its other streams
+// (cudaFree waits for the whole device), and a process whose allocator heap
+// and caching allocator already hold nearly all of HBM, where the bitmap
+// allocation itself fails exactly when a check is most wanted.  For them the
+// bitmap lives in the fixed array below, part of this library's device image:
+// every GPU that loads the library holds its 8 MiB until the process exits.
+// 8 MiB covers 2^26 units of 16 bytes, i.e. heaps of up to 1 GiB of chunk
+// data; larger heaps are refused.
+
+constexpr size_t kNoAllocBitmapWords = OURO_NOALLOC_BITMAP_BYTES / sizeof(uint32_t);
+static __device__ __align__(256) uint32_t ouro_noalloc_bitmap[kNoAllocBitmapWords];
+
+namespace {
+
+// Device address of ouro_noalloc_bitmap on each device.  On the host the
+// array's name is only a stand-in for the device object, so the address is
+// asked from the runtime once per device, with that device current.
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+uint32_t* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+int noalloc_bitmap(int device, uint32_t** out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return OURO_ERR_ARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, ouro_noalloc_bitmap);
+    if (e != cudaSuccess || !p) {
+      (void)cudaGetLastError();
+      return OURO_ERR_CUDA;
+    }
+    g_noalloc_addr[device] = static_cast<uint32_t*>(p);
+  }
+  *out = g_noalloc_addr[device];
+  return OURO_OK;
+}
+
+}  // namespace
+
+int ouro_check_allocations_noalloc(ouro_heap* h, void* const* d_ptrs, uint32_t n, uint32_t size,
+                                   const uint32_t* d_sizes, ouro_alloc_report* d_report, void* stream) {
+  if (!h || !d_ptrs || !d_report) return OURO_ERR_ARG;
+  int device = -1;
+  if (cudaGetDevice(&device) != cudaSuccess) return OURO_ERR_CUDA;
+  if (device != h->device) return OURO_ERR_ARG;
+  const size_t words = (h->L.max_chunks * (kChunkBytes / 16u) + 31u) / 32u;
+  if (words > kNoAllocBitmapWords) return OURO_ERR_TOO_LARGE;
+  uint32_t* bitmap = nullptr;
+  const int rc = noalloc_bitmap(device, &bitmap);
+  if (rc != OURO_OK) return rc;
+  // The array keeps what the previous call left: clear the part this heap
+  // uses, and the caller's report, which the kernel accumulates into.
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(bitmap, 0, words * sizeof(uint32_t), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_report, 0, sizeof(ouro_alloc_report), s);
+  if (e == cudaSuccess && n) {
+    k_check_allocs<<<grid_for(n, 256), 256, 0, s>>>(h->dev, d_ptrs, n, size, d_sizes, bitmap,
+                                                    reinterpret_cast<unsigned long long*>(d_report));
+    e = cudaGetLastError();
+  }
   return cuda_rc(e);
 }
 
