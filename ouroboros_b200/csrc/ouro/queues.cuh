@@ -153,40 +153,46 @@ __device__ void ensure_enqueued(HeapCore* h, ClassState* q, uint32_t c) {
   if (atomicCAS(&h->meta[c].queue_pos, kEmpty, kPending) == kEmpty) chunk_enqueue<Store>(h, q, c);
 }
 
-// The front moves over removed entries; one lane at a time does it (a
+// The front moves over removed entries; one group at a time does it (a
 // try-lock nobody waits on), so removals all over the queue do not turn into
-// thousands of lanes scanning the same run.
+// thousands of groups scanning the same run.  Collective over g.
 template <class Store>
-__device__ void help_front(HeapCore* h, ClassState* q) {
-  if (atomicCAS(&q->advancing.v, 0u, 1u) != 0u) return;
+__device__ void help_front(HeapCore* h, ClassState* q, const Group& g) {
+  uint32_t mine = 0;
+  if (g.is_leader()) mine = atomicCAS(&q->advancing.v, 0u, 1u) == 0u ? 1u : 0u;
+  if (!bcast(g, mine)) return;
 #ifdef OURO_SCAN_STATS
   const long long t0 = clock64();
 #endif
-  Store::advance_front(h, q);
-  __threadfence();
-  atomicExch(&q->advancing.v, 0u);
+  Store::advance_front(h, q, g);
+  __syncwarp(g.mask);
+  if (g.is_leader()) {
+    __threadfence();
+    atomicExch(&q->advancing.v, 0u);
 #ifdef OURO_SCAN_STATS
-  atomicAdd(&h->scan[10].v, 1ull);
-  atomicAdd(&h->scan[11].v, static_cast<unsigned long long>(clock64() - t0));
+    atomicAdd(&h->scan[10].v, 1ull);
+    atomicAdd(&h->scan[11].v, static_cast<unsigned long long>(clock64() - t0));
 #endif
+  }
 }
 
 // Remove the entry of an exhausted chunk (the DEQUEUE_CHUNK mode of
-// ChunkQueue_impl.cuh:128-137) and advance the front over removed entries.
+// ChunkQueue_impl.cuh:128-137).  Called by one lane; returns true when it
+// removed the entry, after which its group should help the front.
 template <class Store>
-__device__ void chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos) {
+__device__ bool chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos) {
   uint32_t* qp = &h->meta[c].queue_pos;
   uint32_t it = 0;
   while (ld_relaxed(qp) == kPending) {
-    if (it >= 4096u) return;
+    if (it >= 4096u) return false;
     backoff(it);
   }
-  if (atomicCAS(qp, pos, kEmpty) != pos) return;   // someone else removed or moved it
+  if (atomicCAS(qp, pos, kEmpty) != pos) return false;   // someone else removed or moved it
   Store::remove(h, q, pos);
   atomicSub(&q->entries.v, 1);
-  help_front<Store>(h, q);
   __threadfence();
   if (ld_relaxed(&h->meta[c].count) > 0) ensure_enqueued<Store>(h, q, c);
+  return true;
 }
 
 // Cooperative claim of `got` free pages of chunk c for the group lanes in
@@ -337,7 +343,7 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
 #define OURO_STAT(x) ((void)0)
 #endif
   for (uint32_t iter = 0;; ++iter) {
-    uint32_t c = kEmpty, got = 0, last = 0;
+    uint32_t c = kEmpty, got = 0, last = 0, help = 0;
     if (s.is_leader()) {
       if (iter > 4u * kSpinLimit) {
         note_timeout(h);
@@ -351,7 +357,7 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
         }
         const uint32_t v = Store::peek(h, q, pos, cur);
         OURO_STAT(st_probe);
-        if (v == kTomb && iter == 0u) help_front<Store>(h, q);   // the front entry is gone
+        if (v == kTomb && iter == 0u) help = 1u;   // the front entry is gone
         const bool live = v < kTomb && v < h->max_chunks && ld_relaxed(&h->meta[v].page_size) == q->page_size;
         if (live && ld_relaxed(&h->meta[v].count) > 0) {
           int32_t old = atomicSub(&h->meta[v].count, static_cast<int32_t>(need));
@@ -373,6 +379,7 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
     }
     c = bcast(s, c);
     if (c == kTomb) return nullptr;   // gave up
+    if (bcast(s, help)) help_front<Store>(h, q, s);
     got = bcast(s, got);
     if (got) {
       last = bcast(s, last);
@@ -387,10 +394,12 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
       t0 = clock64();
 #endif
       if (served && !before) chunk = c;
+      uint32_t removed = 0;
       if (s.is_leader()) {
-        if (last) chunk_dequeue<Store>(h, q, c, pos);
+        if (last) removed = chunk_dequeue<Store>(h, q, c, pos) ? 1u : 0u;
         ++pos;
       }
+      if (bcast(s, removed)) help_front<Store>(h, q, s);
 #ifdef OURO_SCAN_STATS
       t_deq += clock64() - t0;
 #endif
@@ -447,10 +456,11 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
           if (qp != kPending && qp != kEmpty && atomicCAS(&m->queue_pos, qp, kEmpty) == qp) {
             Store::remove(h, q, qp);
             atomicSub(&q->entries.v, 1);
-            help_front<Store>(h, q);
+            flashed = 2u;
+          } else {
+            flashed = 1u;
           }
           reuse_put(h, &h->reuse[q->inst], c);
-          flashed = 1u;
         } else {
           sem_signal(q, static_cast<uint32_t>(size - n));
         }
@@ -458,6 +468,7 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
     }
   }
   flashed = __shfl_sync(cg.mask, flashed, cg.leader);
+  if (flashed == 2u) help_front<Store>(h, q, cg);
   __syncwarp(g.mask);
   __threadfence();
   uint32_t total = __reduce_add_sync(g.mask, flashed ? 0u : 1u);

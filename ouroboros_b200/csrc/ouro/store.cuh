@@ -44,6 +44,46 @@ __device__ __forceinline__ uint32_t take_slot(HeapCore* h, uint32_t* s) {
   return v;
 }
 
+// ------------------------------------------------ front advance (groups)
+// The front of a chunk queue moves over removed entries (kTomb).  One group at
+// a time does it (queues.cuh: help_front): its lanes read 4 consecutive
+// entries each per round with one 16-byte load, so a round covers 4 x group
+// size entries and the first live entry is found with one ballot.  Positions
+// before `from` count as removed, positions at or after `back` as live.
+// Rounds per advance: 256 (32768 entries for a full warp), and at least
+// 8192 entries for small groups.
+__device__ __forceinline__ uint32_t front_rounds(uint32_t n) { return 2048u / n > 256u ? 2048u / n : 256u; }
+
+__device__ __forceinline__ bool first_live4(const Group& g, uint32_t p, uint4 e, uint32_t from, uint32_t back,
+                                            uint32_t* stop) {
+  const uint32_t v[4] = {e.x, e.y, e.z, e.w};
+  uint32_t idx = 4u;
+#pragma unroll
+  for (int k = 3; k >= 0; --k) {
+    const uint32_t pos = p + static_cast<uint32_t>(k);
+    const bool behind = static_cast<int32_t>(pos - from) < 0;
+    const bool beyond = static_cast<int32_t>(pos - back) >= 0;
+    if (!behind && (beyond || v[k] != kTomb)) idx = static_cast<uint32_t>(k);
+  }
+  const uint32_t m = __ballot_sync(g.mask, idx < 4u);
+  if (!m) return false;
+  *stop = __shfl_sync(g.mask, p + idx, __ffs(m) - 1);
+  return true;
+}
+
+// Claim [from, stop) for the front with one CAS (from = the front we read).
+// Returns the start of the part this group moved the front over (== stop when
+// another group got at least as far).
+__device__ __forceinline__ uint32_t claim_front(ClassState* q, uint32_t from, uint32_t stop) {
+  uint32_t cur = from;
+  for (;;) {
+    const uint32_t seen = atomicCAS(&q->front.v, cur, stop);
+    if (seen == cur) return cur;
+    if (static_cast<int32_t>(seen - stop) >= 0) return stop;   // someone else moved it at least as far
+    cur = seen;                                                 // [seen, stop) is still ours to pass
+  }
+}
+
 // ================================================================= flat
 struct FlatStore {
   static constexpr int kKind = 0;
@@ -93,22 +133,35 @@ struct FlatStore {
   __device__ static void remove(HeapCore* h, ClassState* q, uint32_t pos) { st_relaxed(slot(q, pos), kTomb); }
 
   // Move the front past removed entries, freeing their slots for the next lap.
-  // The removed run is found with plain loads and claimed with one CAS, so
-  // many lanes finishing chunks at once do not fight over the front word.
-  __device__ static void advance_front(HeapCore* h, ClassState* q) {
-    const uint32_t f = ld_relaxed(&q->front.v);
-    const uint32_t back = ld_relaxed(&q->back.v);
-    uint32_t g = f;
-    while (g != back && g - f < 8192u && ld_relaxed(slot(q, g)) == kTomb) ++g;
-    if (g == f) return;
-    uint32_t cur = f;
-    for (;;) {
-      const uint32_t seen = atomicCAS(&q->front.v, cur, g);
-      if (seen == cur) break;
-      if (static_cast<int32_t>(seen - g) >= 0) return;   // someone else moved it at least as far
-      cur = seen;                                         // [seen, g) is still ours to pass
+  __device__ static void advance_front(HeapCore* h, ClassState* q, const Group& g) {
+    uint32_t f = 0, back = 0;
+    if (g.is_leader()) {
+      f = ld_relaxed(&q->front.v);
+      back = ld_relaxed(&q->back.v);
     }
-    for (uint32_t p = cur; p != g; ++p) st_relaxed(slot(q, p), kEmpty);
+    f = bcast(g, f);
+    back = bcast(g, back);
+    if (static_cast<int32_t>(back - f) <= 0) return;
+    const uint32_t n = static_cast<uint32_t>(g.size);
+    uint32_t a = f & ~3u, stop = 0;
+    bool found = false;
+    for (uint32_t r = 0, rounds = front_rounds(n); r < rounds && !found; ++r, a += 4u * n) {
+      const uint32_t p = a + 4u * static_cast<uint32_t>(g.rank);
+      // ring positions are 4-aligned here and the ring size is a multiple of 4
+      const uint4 e = static_cast<int32_t>(p - back) < 0 ? ld_relaxed_v4(slot(q, p)) : make_uint4(0, 0, 0, 0);
+      found = first_live4(g, p, e, f, back, &stop);
+      if (!found && static_cast<int32_t>(a + 4u * n - back) >= 0) {
+        stop = back;
+        found = true;
+      }
+    }
+    if (!found) stop = a;
+    if (static_cast<int32_t>(stop - f) <= 0) return;
+    uint32_t cur = 0;
+    if (g.is_leader()) cur = claim_front(q, f, stop);
+    cur = bcast(g, cur);
+    for (uint32_t p = cur + static_cast<uint32_t>(g.rank); p != stop && static_cast<int32_t>(p - stop) < 0; p += n)
+      st_relaxed(slot(q, p), kEmpty);
   }
 };
 
@@ -258,35 +311,56 @@ struct VaStore {
     atomicSub(&h->meta[qc].qcount, 1u << 16);
   }
   // Front moves over removed entries; passing the last entry of a queue chunk
-  // returns that chunk to the pool (ChunkQueueVA_impl.cuh:144-156).  Same
-  // scan-then-one-CAS scheme as the flat ring.
-  __device__ static void advance_front(HeapCore* h, ClassState* q) {
-    const uint32_t f = ld_relaxed(&q->front.v);
-    const uint32_t back = ld_relaxed(&q->back.v);
-    uint32_t g = f, qc = kEmpty;
-    while (g != back && g - f < 8192u) {
-      if (g == f || g % kQcSpots == 0u) {
-        qc = ld_acquire(q->ring + vid(g));
-        if (qc >= kInstalling || ld_relaxed(&h->meta[qc].vstart) / kQcSpots != g / kQcSpots) break;
-      }
-      if (ld_acquire(queue_slots(h, qc) + (g % kQcSpots)) != kTomb) break;
-      ++g;
+  // returns that chunk to the pool (ChunkQueueVA_impl.cuh:144-156).  Each lane
+  // keeps the queue chunk of its own positions and looks the next one up when
+  // it crosses a 2048-entry boundary; a missing or reused queue chunk stops
+  // the scan.
+  __device__ static void advance_front(HeapCore* h, ClassState* q, const Group& g) {
+    uint32_t f = 0, back = 0;
+    if (g.is_leader()) {
+      f = ld_relaxed(&q->front.v);
+      back = ld_relaxed(&q->back.v);
     }
-    if (g == f) return;
-    uint32_t cur = f;
-    for (;;) {
-      const uint32_t seen = atomicCAS(&q->front.v, cur, g);
-      if (seen == cur) break;
-      if (static_cast<int32_t>(seen - g) >= 0) return;
-      cur = seen;
-    }
-    // every queue chunk whose last entry lies in [cur, g) is now behind the front
-    for (uint32_t end = cur - cur % kQcSpots + kQcSpots; static_cast<int32_t>(g - end) >= 0; end += kQcSpots) {
-      const uint32_t c = atomicExch(q->ring + vid(end - 1u), kEmpty);
-      if (c < kInstalling) {
-        clean_queue_chunk(h, c);
-        reuse_put(h, &h->reuse[0], c);
+    f = bcast(g, f);
+    back = bcast(g, back);
+    if (static_cast<int32_t>(back - f) <= 0) return;
+    const uint32_t n = static_cast<uint32_t>(g.size);
+    uint32_t a = f & ~3u, stop = 0, range = kEmpty, qc = kEmpty;
+    bool found = false;
+    for (uint32_t r = 0, rounds = front_rounds(n); r < rounds && !found; ++r, a += 4u * n) {
+      const uint32_t p = a + 4u * static_cast<uint32_t>(g.rank);
+      uint4 e = make_uint4(0, 0, 0, 0);
+      if (static_cast<int32_t>(p - back) < 0) {
+        if (p / kQcSpots != range) {
+          range = p / kQcSpots;
+          qc = ld_acquire(q->ring + vid(p));
+          if (qc >= kInstalling || ld_relaxed(&h->meta[qc].vstart) / kQcSpots != range) qc = kEmpty;
+        }
+        if (qc != kEmpty) e = ld_relaxed_v4(queue_slots(h, qc) + (p % kQcSpots));
       }
+      found = first_live4(g, p, e, f, back, &stop);
+      if (!found && static_cast<int32_t>(a + 4u * n - back) >= 0) {
+        stop = back;
+        found = true;
+      }
+    }
+    if (!found) stop = a;
+    if (static_cast<int32_t>(stop - f) <= 0) return;
+    uint32_t cur = 0;
+    if (g.is_leader()) cur = claim_front(q, f, stop);
+    cur = bcast(g, cur);
+    // every queue chunk whose last entry lies in [cur, stop) is now behind the front
+    for (uint32_t end = cur - cur % kQcSpots + kQcSpots; static_cast<int32_t>(stop - end) >= 0; end += kQcSpots) {
+      uint32_t c = kEmpty;
+      if (g.is_leader()) c = atomicExch(q->ring + vid(end - 1u), kEmpty);
+      c = bcast(g, c);
+      if (c >= kInstalling) continue;
+      uint32_t* slots = queue_slots(h, c);
+      const uint4 empty = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
+      for (uint32_t i = 4u * static_cast<uint32_t>(g.rank); i < kQcSpots; i += 4u * n) st_v4(slots + i, empty);
+      __syncwarp(g.mask);
+      __threadfence();
+      if (g.is_leader()) reuse_put(h, &h->reuse[0], c);
     }
   }
 };
@@ -593,38 +667,67 @@ struct VlStore {
     __threadfence();
     count_removed(h, q, qc, 1u);
   }
-  __device__ static void advance_front(HeapCore* h, ClassState* q) {
-    const uint32_t f = ld_relaxed(&q->front.v);
-    const uint32_t back = ld_relaxed(&q->back.v);
-    if (static_cast<int32_t>(back - f) <= 0) return;
-    const uint32_t first = ld_acquire(&q->front_ptr);
-    uint32_t qc = locate(h, first, f);
-    if (qc == kEmpty) return;
-    uint32_t g = f;
-    if (qc == kBehind) {
-      // front lags the first live queue chunk: everything before it is gone
-      const uint32_t vs = ld_relaxed(&h->meta[first].vstart);
-      g = vs - vs % kQcSpots;
-      qc = first;
-    }
-    uint32_t range = g / kQcSpots;   // virtual queue chunk that qc holds
-    while (g != back && g - f < 8192u) {
-      if (g / kQcSpots != range) {
-        const uint32_t nx = ld_acquire(&h->meta[qc].next);
-        if (nx >= kInstalling) break;
-        qc = nx;
-        range = g / kQcSpots;
+  // Front moves over removed entries.  The leader walks the chain: per round
+  // the group's positions span at most two queue chunks (4 x 32 < 2048), the
+  // current one and its successor.  Drained queue chunks leave the chain
+  // through count_removed / set_front, not here.
+  __device__ static void advance_front(HeapCore* h, ClassState* q, const Group& g) {
+    uint32_t f = 0, back = 0, qc = kEmpty, from = 0;
+    if (g.is_leader()) {
+      f = ld_relaxed(&q->front.v);
+      back = ld_relaxed(&q->back.v);
+      from = f;
+      if (static_cast<int32_t>(back - f) > 0) {
+        const uint32_t first = ld_acquire(&q->front_ptr);
+        qc = locate(h, first, f);
+        if (qc == kBehind) {
+          // front lags the first live queue chunk: everything before it is gone
+          const uint32_t vs = ld_relaxed(&h->meta[first].vstart);
+          from = vs - vs % kQcSpots;
+          qc = first;
+        }
       }
-      if (ld_acquire(queue_slots(h, qc) + (g % kQcSpots)) != kTomb) break;
-      ++g;
     }
-    if (static_cast<int32_t>(g - f) <= 0) return;
-    uint32_t cur = f;
-    for (;;) {
-      const uint32_t seen = atomicCAS(&q->front.v, cur, g);
-      if (seen == cur || static_cast<int32_t>(seen - g) >= 0) return;
-      cur = seen;
+    f = bcast(g, f);
+    back = bcast(g, back);
+    from = bcast(g, from);
+    qc = bcast(g, qc);
+    if (static_cast<int32_t>(back - f) <= 0 || qc == kEmpty) return;
+    const uint32_t n = static_cast<uint32_t>(g.size);
+    uint32_t a = from & ~3u, stop = 0, range = from / kQcSpots;   // range: the virtual queue chunk qc holds
+    bool found = false;
+    for (uint32_t r = 0, rounds = front_rounds(n); r < rounds && !found; ++r, a += 4u * n) {
+      if (a / kQcSpots != range) {   // the round starts in the next queue chunk
+        uint32_t nx = kEmpty;
+        if (g.is_leader()) nx = ld_acquire(&h->meta[qc].next);
+        nx = bcast(g, nx);
+        if (nx >= kInstalling) {
+          stop = a;
+          found = true;
+          break;
+        }
+        qc = nx;
+        range = a / kQcSpots;
+      }
+      uint32_t nx = kEmpty;   // successor, for lanes past the end of qc
+      if ((a + 4u * n - 1u) / kQcSpots != range) {
+        if (g.is_leader()) nx = ld_acquire(&h->meta[qc].next);
+        nx = bcast(g, nx);
+      }
+      const uint32_t p = a + 4u * static_cast<uint32_t>(g.rank);
+      const uint32_t mine = p / kQcSpots == range ? qc : nx;
+      uint4 e = make_uint4(0, 0, 0, 0);
+      if (static_cast<int32_t>(p - back) < 0 && mine < kInstalling)
+        e = ld_relaxed_v4(queue_slots(h, mine) + (p % kQcSpots));
+      found = first_live4(g, p, e, from, back, &stop);
+      if (!found && static_cast<int32_t>(a + 4u * n - back) >= 0) {
+        stop = back;
+        found = true;
+      }
     }
+    if (!found) stop = a;
+    if (static_cast<int32_t>(stop - f) <= 0) return;
+    if (g.is_leader()) claim_front(q, f, stop);
   }
 };
 
