@@ -39,7 +39,7 @@ __global__ void k_init_queues(Ouroboros<V>* mm) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (uint32_t cls = 0; cls < kNumClasses; ++cls) {
     ClassState* q = &mm->cls[cls];
-    uint32_t c = new_queue_chunk(mm, q->inst, 0u);
+    uint32_t c = new_queue_chunk(mm, q->inst, 0u, queue_tag(q));
     if (c == kEmpty) return;
     if constexpr (Ouroboros<V>::kKind == 1) {
       st_relaxed(q->ring, c);

@@ -37,7 +37,8 @@ struct alignas(128) ClassState {
   Line<uint32_t> back;            // producer position (virtual)
   Line<int32_t> entries;          // chunk-based: entries in the queue (count_)
   Line<uint32_t> cursor;          // chunk-based: next-fit scan cursor for contended groups
-  Line<uint32_t> advancing;       // chunk-based: try-lock of the lane moving the front
+  Line<uint32_t> advancing;       // chunk-based: try-lock of the group moving the front
+  Line<uint32_t> ptr_lock;        // linked: try-lock of the group moving front_ptr / old_ptr
   // cold line
   uint32_t* ring;                 // standard: the ring; virtualized array: the index array
   uint32_t ring_mask;
@@ -231,9 +232,10 @@ __device__ inline uint32_t alloc_chunks(HeapCore* h, const Group& g, uint32_t k,
 // entry kEmpty as they drain, and chunk queues clean a queue chunk when they
 // return it to the pool (clean_queue_chunk).  This keeps the 8 KiB rewrite
 // off the path where producers wait for the next queue chunk.
-__device__ inline void init_queue_chunk(HeapCore* h, uint32_t c, uint32_t vstart) {
+__device__ inline void init_queue_chunk(HeapCore* h, uint32_t c, uint32_t vstart, uint32_t tag) {
   ChunkMeta* m = h->meta + c;
   st_relaxed(&m->page_size, 0u);
+  st_relaxed(&m->size, tag);
   st_relaxed(&m->head, 0u);
   st_relaxed(&m->qcount, 0u);
   st_relaxed(&m->vstart, vstart);
@@ -255,7 +257,13 @@ __device__ __forceinline__ uint32_t* queue_slots(HeapCore* h, uint32_t c) {
 }
 
 // One lane allocates one queue chunk (allocateChunk<true>) and initializes it.
-__device__ inline uint32_t new_queue_chunk(HeapCore* h, uint32_t inst, uint32_t vstart);
+__device__ inline uint32_t new_queue_chunk(HeapCore* h, uint32_t inst, uint32_t vstart, uint32_t tag);
+
+// Owner tag of a class's queue chunks, kept in ChunkMeta::size (data chunks
+// hold their page count there, at most 512; recycled queue chunks 0): an index
+// entry is trusted only for a chunk that still carries its class's tag.
+constexpr uint32_t kQueueTag = 0x40000000u;
+__device__ __forceinline__ uint32_t queue_tag(const ClassState* q) { return kQueueTag | q->cls; }
 
 // Link slot of a queue chunk (a virtual-array index entry or a `next` field):
 // the pre-allocating lane offers its chunk with a CAS; if a waiting lane got
@@ -267,18 +275,19 @@ __device__ inline void offer_queue_chunk(HeapCore* h, uint32_t* link, uint32_t n
 
 // A lane that has waited long for a link installs a queue chunk itself.
 // Returns true when the link is now set (by anyone).
-__device__ inline void install_queue_chunk(HeapCore* h, uint32_t* link, uint32_t inst, uint32_t vstart) {
+__device__ inline void install_queue_chunk(HeapCore* h, uint32_t* link, uint32_t inst, uint32_t vstart,
+                                           uint32_t tag) {
   if (atomicCAS(link, kEmpty, kInstalling) != kEmpty) return;
-  uint32_t nq = new_queue_chunk(h, inst, vstart);
+  uint32_t nq = new_queue_chunk(h, inst, vstart, tag);
   st_release(link, nq);   // kEmpty again when no chunk was free: someone retries later
 }
 
-__device__ inline uint32_t new_queue_chunk(HeapCore* h, uint32_t inst, uint32_t vstart) {
+__device__ inline uint32_t new_queue_chunk(HeapCore* h, uint32_t inst, uint32_t vstart, uint32_t tag) {
   Group self = make_group(1u << lane_id());
   uint32_t c;
   uint32_t got = alloc_chunks(h, self, 1u, inst, true, &c);
   if (!got || c == kEmpty) return kEmpty;
-  init_queue_chunk(h, c, vstart);
+  init_queue_chunk(h, c, vstart, tag);
   __threadfence();
   return c;
 }

@@ -90,7 +90,13 @@ __device__ uint32_t page_grow(HeapCore* h, ClassState* q, const Group& g, uint32
 
 template <class Store>
 __device__ void* page_alloc(HeapCore* h, ClassState* q, const Group& g) {
+#ifdef OURO_SCAN_STATS
+  const long long t0 = clock64();
+#endif
   uint32_t granted = sem_acquire(h, q, g, [&](uint32_t k) { return page_grow<Store>(h, q, g, k); });
+#ifdef OURO_SCAN_STATS
+  const long long t1 = clock64();
+#endif
   const bool served = static_cast<uint32_t>(g.rank) < granted;
   if (granted < static_cast<uint32_t>(g.size) && g.is_leader()) {
     atomicAdd(&h->oom.v, static_cast<unsigned long long>(g.size - granted));
@@ -103,6 +109,16 @@ __device__ void* page_alloc(HeapCore* h, ClassState* q, const Group& g) {
   if (s.is_leader()) t = atomicAdd(&q->front.v, granted);
   t = bcast(s, t);
   uint32_t v = Store::consume_lane(h, q, s, t + static_cast<uint32_t>(s.rank));
+#ifdef OURO_SCAN_STATS
+  if (s.is_leader()) {
+    const long long t2 = clock64();
+    atomicAdd(&h->scan[0].v, 1ull);
+    atomicAdd(&h->scan[1].v, static_cast<unsigned long long>(t1 - t0));
+    atomicAdd(&h->scan[2].v, static_cast<unsigned long long>(t2 - t1));
+    if (t2 - t0 > (1ll << 20)) atomicAdd(&h->scan[8].v, 1ull);
+    atomicMax(&h->scan[9].v, static_cast<unsigned long long>(t2 - t0));
+  }
+#endif
   if (v == kEmpty) return nullptr;
   return page_address(h, v >> kPageBits, v & ((1u << kPageBits) - 1u), q->page_shift);
 }
@@ -111,6 +127,9 @@ __device__ void* page_alloc(HeapCore* h, ClassState* q, const Group& g) {
 template <class Store>
 __device__ void page_free(HeapCore* h, ClassState* q, const Group& g, uint32_t index) {
   __threadfence();   // the caller's writes to the page are visible before it is handed out again
+#ifdef OURO_SCAN_STATS
+  const long long t0 = clock64();
+#endif
   uint32_t b = 0;
   if (g.is_leader()) b = atomicAdd(&q->back.v, static_cast<uint32_t>(g.size));
   b = bcast(g, b);
@@ -118,6 +137,14 @@ __device__ void page_free(HeapCore* h, ClassState* q, const Group& g, uint32_t i
   __syncwarp(g.mask);
   __threadfence();
   if (g.is_leader()) sem_signal(q, static_cast<uint32_t>(g.size));
+#ifdef OURO_SCAN_STATS
+  if (g.is_leader()) {
+    const long long t1 = clock64();
+    atomicAdd(&h->scan[4].v, 1ull);
+    atomicAdd(&h->scan[5].v, static_cast<unsigned long long>(t1 - t0));
+    atomicMax(&h->scan[6].v, static_cast<unsigned long long>(t1 - t0));
+  }
+#endif
 }
 
 // =========================================================== chunk queues

@@ -178,7 +178,7 @@ struct VaStore {
     while ((c = ld_acquire(e)) == kEmpty || c == kInstalling) {
       if (it >= kSpinLimit) { note_timeout(h); return kEmpty; }
       if (c == kEmpty && it >= kInstallAfter && (it & 63u) == 0u)
-        install_queue_chunk(h, e, q->inst, pos - pos % kQcSpots);
+        install_queue_chunk(h, e, q->inst, pos - pos % kQcSpots, queue_tag(q));
       backoff(it);
     }
     if (ld_relaxed(&h->meta[c].vstart) / kQcSpots != pos / kQcSpots) {
@@ -191,7 +191,7 @@ struct VaStore {
   // The producer of a position at the start of a queue chunk allocates the
   // next queue chunk (PageQueueVA_impl.cuh:45-56, :202-212).
   __device__ static void preallocate(HeapCore* h, ClassState* q, uint32_t pos) {
-    offer_queue_chunk(h, q->ring + vid(pos + kQcSpots), new_queue_chunk(h, q->inst, pos + kQcSpots));
+    offer_queue_chunk(h, q->ring + vid(pos + kQcSpots), new_queue_chunk(h, q->inst, pos + kQcSpots, queue_tag(q)));
   }
 
   // Drained queue chunk back to the chunk pool (PageQueueVA_impl.cuh:159-166).
@@ -371,15 +371,21 @@ struct VlStore {
   static constexpr uint32_t kBehind = 0xFFFFFFFDu;
 
   // Direct-mapped index of recently linked queue chunks (virtual chunk id mod
-  // kSkipSlots).  An entry is only a hint, valid when the chunk's vstart
-  // matches; it turns the pointer chase of a burst into one lookup.
+  // kSkipSlots).  An entry is only a hint, valid while the chunk carries the
+  // class's queue tag and the range; it turns the pointer chase of a burst
+  // into one lookup.
   __device__ static void remember(HeapCore* h, ClassState* q, uint32_t c, uint32_t vstart) {
     st_relaxed(q->skip + ((vstart / kQcSpots) & (kSkipSlots - 1u)), c);
   }
-  __device__ static uint32_t recall(HeapCore* h, ClassState* q, uint32_t pos) {
-    const uint32_t c = ld_relaxed(q->skip + ((pos / kQcSpots) & (kSkipSlots - 1u)));
-    if (c < h->max_chunks && ld_relaxed(&h->meta[c].vstart) / kQcSpots == pos / kQcSpots) return c;
+  __device__ static uint32_t recall_range(HeapCore* h, ClassState* q, uint32_t range) {
+    const uint32_t c = ld_relaxed(q->skip + (range & (kSkipSlots - 1u)));
+    if (c < h->max_chunks && ld_relaxed(&h->meta[c].size) == queue_tag(q) &&
+        ld_relaxed(&h->meta[c].vstart) / kQcSpots == range)
+      return c;
     return kEmpty;
+  }
+  __device__ static uint32_t recall(HeapCore* h, ClassState* q, uint32_t pos) {
+    return recall_range(h, q, pos / kQcSpots);
   }
 
   // Walk from `from` to the queue chunk holding pos (QueueChunk_impl.cuh:403-426).
@@ -389,6 +395,9 @@ struct VlStore {
     for (uint32_t hops = 0; hops < (1u << 20); ++hops) {
       uint32_t vs = ld_relaxed(&h->meta[cur].vstart) / kQcSpots;
       uint32_t want = pos / kQcSpots;
+#ifdef OURO_SCAN_STATS
+      if (vs == want) atomicAdd(&h->scan[7].v, static_cast<unsigned long long>(hops));
+#endif
       if (vs == want) return cur;
       if (static_cast<int32_t>(want - vs) < 0) return kBehind;
       uint32_t nx = next_of(h, cur, it);
@@ -403,6 +412,9 @@ struct VlStore {
   // meanwhile), trying the index first.
   __device__ static uint32_t locate_live(HeapCore* h, ClassState* q, uint32_t from, uint32_t pos) {
     const uint32_t c = recall(h, q, pos);
+#ifdef OURO_SCAN_STATS
+    if (c == kEmpty) atomicAdd(&h->scan[3].v, 1ull);
+#endif
     return c != kEmpty ? c : locate(h, from, pos);
   }
 
@@ -416,7 +428,8 @@ struct VlStore {
       if (it >= kSpinLimit) { note_timeout(h); return kEmpty; }
       if (nx == kEmpty && it >= kInstallAfter && (it & 63u) == 0u) {
         uint32_t vs = ld_relaxed(&h->meta[c].vstart);
-        install_queue_chunk(h, link, 0u, vs - vs % kQcSpots + kQcSpots);   // queue chunks always come from the base pool
+        install_queue_chunk(h, link, 0u, vs - vs % kQcSpots + kQcSpots,   // queue chunks always come from the base pool
+                            ld_relaxed(&h->meta[c].size));
       }
       backoff(it);
     }
@@ -427,120 +440,237 @@ struct VlStore {
     return next_of(h, c, it);
   }
 
-  // QueueChunk_impl.cuh:440-463 setBackPointer.  Called when cur is full, so
-  // its link exists or is about to (its first producer pre-allocates it).
-  __device__ static void set_back(HeapCore* h, ClassState* q, uint32_t cur) {
-    for (uint32_t i = 0; i < (1u << 16); ++i) {
-      uint32_t nx = next_of(h, cur);
-      if (nx == kEmpty) return;
-      if (atomicCAS(&q->back_ptr, cur, nx) != cur) return;
-      if ((ld_relaxed(&h->meta[nx].qcount) & 0xFFFFu) == kQcSpots) cur = nx;
-      else return;
+  // QueueChunk_impl.cuh:440-463 setBackPointer.  back_ptr, where locate()
+  // starts for producers, moves over full queue chunks whose successor is
+  // linked.  Every walk starts from the current back_ptr and publishes with
+  // one CAS, so a chunk that fills while another lane walks is passed by one
+  // of the two.
+  __device__ static void set_back(HeapCore* h, ClassState* q) {
+    uint32_t bp = ld_acquire(&q->back_ptr);
+    for (uint32_t round = 0; round < 64u; ++round) {
+      uint32_t cur = bp;
+      for (uint32_t i = 0; i < (1u << 16); ++i) {
+        if ((ld_acquire(&h->meta[cur].qcount) & 0xFFFFu) != kQcSpots) break;
+        const uint32_t nx = ld_acquire(&h->meta[cur].next);
+        if (nx >= kInstalling) break;
+        cur = nx;
+      }
+      if (cur == bp) return;
+      const uint32_t seen = atomicCAS(&q->back_ptr, bp, cur);
+      if (seen == bp) return;
+      bp = seen;   // moved by someone else: walk on from there
     }
   }
 
-  // QueueChunk_impl.cuh:467-490 setFrontPointer
-  __device__ static uint32_t set_front(HeapCore* h, ClassState* q, uint32_t cur) {
-    uint32_t ret = 0;
-    for (uint32_t i = 0; i < (1u << 16); ++i) {
-      uint32_t nx = next_of(h, cur);
-      if (nx == kEmpty) break;
-      if (atomicCAS(&q->front_ptr, cur, nx) != cur) break;
-      ++ret;
-      if (ld_relaxed(&h->meta[nx].qcount) == kQcSpots) cur = nx;
-      else break;
-    }
-    return ret;
+  // Rank of the lowest lane of m within the group.
+  __device__ static uint32_t first_rank(const Group& g, uint32_t m) {
+    return static_cast<uint32_t>(__popc(g.mask & ((1u << (__ffs(m) - 1)) - 1u)));
   }
 
-  // QueueChunk_impl.cuh:494-551 setOldPointer: drained chunks are held back
-  // (up to kOldHold) before they return to the pool, so that a lane that read
-  // front/back a little while ago can still walk forward from it.
-  __device__ static void set_old(HeapCore* h, ClassState* q, uint32_t freed) {
-    uint32_t cur = ld_relaxed(&q->old_count);
-    if (cur < kOldHold) {
-      cur = atomicAdd(&q->old_count, freed);
-      if (cur < kOldHold) {
-        if (cur + freed > kOldHold) {
-          freed = cur + freed - kOldHold;
-          atomicSub(&q->old_count, freed);
-        } else {
-          freed = 0;
+  // From chunk fp on, the queue chunks that are drained (all 2048 entries
+  // taken) and linked to a successor.  Lane r looks up the chunk of range
+  // (fp's range + r) in the index and checks that it is the successor of
+  // rank r-1's chunk, so a round covers up to one chunk per lane; an index
+  // miss ends the round early.  Returns how many chunks can be passed and
+  // moves *fp to the first one that cannot.  Collective over g.
+  __device__ static uint32_t walk_drained(HeapCore* h, ClassState* q, const Group& g, uint32_t* fp_io) {
+    const uint32_t n = static_cast<uint32_t>(g.size), r = static_cast<uint32_t>(g.rank);
+    uint32_t fp = *fp_io, passed = 0;
+    uint32_t range = ld_relaxed(&h->meta[fp].vstart) / kQcSpots;
+    for (uint32_t round = 0; round < (1u << 16); ++round) {
+      const uint32_t c = r == 0u ? fp : recall_range(h, q, range + r);
+      uint32_t cnt = 0, nx = kEmpty;
+      if (c != kEmpty) {
+        cnt = ld_acquire(&h->meta[c].qcount);
+        nx = ld_acquire(&h->meta[c].next);
+      }
+      const uint32_t prev_nx = __shfl_sync(g.mask, nx, lane_of_rank(g.mask, r == 0u ? 0 : static_cast<int>(r) - 1));
+      const bool linked = r == 0u || (c != kEmpty && c == prev_nx);
+      const bool pass = linked && cnt == kQcSpots && nx < kInstalling;
+      const uint32_t stop_m = __ballot_sync(g.mask, !pass);
+      const uint32_t k = stop_m ? first_rank(g, stop_m) : n;
+      if (k == 0u) break;
+      fp = __shfl_sync(g.mask, nx, lane_of_rank(g.mask, static_cast<int>(k) - 1));
+      passed += k;
+      range += k;
+      if (k < n && __shfl_sync(g.mask, linked ? 1u : 0u, lane_of_rank(g.mask, static_cast<int>(k)))) break;
+    }
+    *fp_io = fp;
+    return passed;
+  }
+
+  // Return k chained queue chunks starting at c to the base pool: lanes find
+  // their chunk as in walk_drained, clear its tag and page size (and its
+  // entries for chunk queues), and all of a round are published with one
+  // reservation on the reuse ring.  Returns the chunk after the last one.
+  // Collective over g.
+  __device__ static uint32_t recycle_run(HeapCore* h, ClassState* q, const Group& g, uint32_t c, uint32_t k) {
+    const uint32_t n = static_cast<uint32_t>(g.size), r = static_cast<uint32_t>(g.rank);
+    ReuseQueue* rq = &h->reuse[0];
+    uint32_t range = ld_relaxed(&h->meta[c].vstart) / kQcSpots;
+    for (uint32_t guard = 0; k > 0u && guard < (1u << 16); ++guard) {
+      const uint32_t want = k < n ? k : n;
+      uint32_t mine = kEmpty, nx = kEmpty;
+      if (r < want) {
+        mine = r == 0u ? c : recall_range(h, q, range + r);
+        if (mine != kEmpty) nx = ld_acquire(&h->meta[mine].next);
+      }
+      const uint32_t prev_nx = __shfl_sync(g.mask, nx, lane_of_rank(g.mask, r == 0u ? 0 : static_cast<int>(r) - 1));
+      const bool ok = r < want && (r == 0u || (mine != kEmpty && mine == prev_nx)) && nx < kInstalling;
+      const uint32_t bad = __ballot_sync(g.mask, !ok);
+      const uint32_t L = bad ? first_rank(g, bad) : n;
+      if (L == 0u) {   // a chunk behind front_ptr without a successor: the chain is broken
+        if (g.is_leader()) set_status(h, kErrCorrupt);
+        break;
+      }
+      const uint32_t after = __shfl_sync(g.mask, nx, lane_of_rank(g.mask, static_cast<int>(L) - 1));
+      if (r < L) {
+        if (q->clean_on_recycle) clean_queue_chunk(h, mine);
+        st_relaxed(&h->meta[mine].size, 0u);
+        st_relaxed(&h->meta[mine].page_size, 0u);
+        __threadfence();
+      }
+      __syncwarp(g.mask);
+      uint32_t pos = 0, take = L;
+      if (g.is_leader()) {
+        const int32_t fill = atomicAdd(&rq->count.v, static_cast<int32_t>(L));
+        if (fill + static_cast<int32_t>(L) > static_cast<int32_t>(kReuseSize)) {
+          take = fill >= static_cast<int32_t>(kReuseSize) ? 0u : kReuseSize - static_cast<uint32_t>(fill);
+          atomicSub(&rq->count.v, static_cast<int32_t>(L - take));
+          set_status(h, kErrQueueFull);   // those chunks stay out of circulation
+        }
+        if (take) pos = atomicAdd(&rq->back.v, take);
+      }
+      pos = bcast(g, pos);
+      take = bcast(g, take);
+      if (r < take) {
+        uint32_t* sl = rq->ring + ((pos + r) & (kReuseSize - 1u));
+        if (wait_slot_empty(h, sl)) st_release(sl, mine);
+      }
+      c = after;
+      range += L;
+      k -= L;
+    }
+    return c;
+  }
+
+  // QueueChunk_impl.cuh:467-551 setFrontPointer + setOldPointer.  One group
+  // at a time (try-lock on the class's ptr_lock line) moves front_ptr over
+  // every drained queue chunk whose successor is linked and returns the
+  // drained chunks more than kOldHold behind it to the pool -- held back so
+  // that a lane that read front_ptr a little while ago can still walk forward
+  // from it.  A group that finds the lock taken returns: the holder re-checks
+  // the chunk at front_ptr after unlocking, so no drain is lost.  Collective
+  // over g.
+  __device__ static void on_empty(HeapCore* h, ClassState* q, const Group& g) {
+    for (uint32_t round = 0; round < 64u; ++round) {
+      uint32_t mine = 0;
+      if (g.is_leader()) mine = atomicCAS(&q->ptr_lock.v, 0u, 1u) == 0u ? 1u : 0u;
+      if (!bcast(g, mine)) return;
+      __threadfence();
+      uint32_t fp = 0, held = 0, old = 0;
+      if (g.is_leader()) {
+        fp = ld_relaxed(&q->front_ptr);
+        held = ld_relaxed(&q->old_count);
+        old = ld_relaxed(&q->old_ptr);
+      }
+      fp = bcast(g, fp);
+      held = bcast(g, held);
+      old = bcast(g, old);
+      const uint32_t passed = walk_drained(h, q, g, &fp);
+      if (passed) {
+        if (g.is_leader()) st_release(&q->front_ptr, fp);
+        held += passed;
+        if (held > kOldHold) {
+          old = recycle_run(h, q, g, old, held - kOldHold);
+          held = kOldHold;
+        }
+        if (g.is_leader()) {
+          st_relaxed(&q->old_ptr, old);
+          st_relaxed(&q->old_count, held);
         }
       }
-    }
-    uint32_t old = ld_relaxed(&q->old_ptr);
-    for (uint32_t guard = 0; freed > 0 && guard < (1u << 20); ++guard) {
-      uint32_t nx = ld_acquire(&h->meta[old].next);
-      if (nx >= kInstalling) break;
-      uint32_t seen = atomicCAS(&q->old_ptr, old, nx);
-      if (seen == old) {
-        --freed;
-        if (q->clean_on_recycle) clean_queue_chunk(h, old);
-        reuse_put(h, &h->reuse[0], old);
-        old = nx;
-      } else {
-        old = seen;
+      __syncwarp(g.mask);
+      uint32_t again = 0;
+      if (g.is_leader()) {
+        __threadfence();
+        atomicExch(&q->ptr_lock.v, 0u);
+        const uint32_t f2 = ld_acquire(&q->front_ptr);
+        again = ld_acquire(&h->meta[f2].qcount) == kQcSpots && ld_acquire(&h->meta[f2].next) < kInstalling ? 1u : 0u;
       }
+      if (!bcast(g, again)) return;
     }
-  }
-
-  __device__ static void on_empty(HeapCore* h, ClassState* q, uint32_t c) {
-    uint32_t n = set_front(h, q, c);
-    set_old(h, q, n);
   }
 
   // Count update of m enqueued entries into chunk c (QueueChunk_impl.cuh:160-182).
-  __device__ static void count_enqueued(HeapCore* h, ClassState* q, uint32_t c, uint32_t m) {
+  // Returns true when this update completes the chunk's drain: the caller's
+  // group then runs on_empty.
+  __device__ static bool count_enqueued(HeapCore* h, ClassState* q, uint32_t c, uint32_t m) {
     uint32_t add = (m << 16) + m;
     uint32_t old = atomicAdd(&h->meta[c].qcount, add);
-    if ((old & 0xFFFFu) + m == kQcSpots) set_back(h, q, c);
-    if (old + add == kQcSpots) on_empty(h, q, c);
+    if ((old & 0xFFFFu) + m == kQcSpots) set_back(h, q);
+    return old + add == kQcSpots;
   }
 
-  __device__ static void count_removed(HeapCore* h, ClassState* q, uint32_t c, uint32_t m) {
+  __device__ static bool count_removed(HeapCore* h, ClassState* q, uint32_t c, uint32_t m) {
     uint32_t sub = m << 16;
     uint32_t old = atomicSub(&h->meta[c].qcount, sub);
-    if (old - sub == kQcSpots) on_empty(h, q, c);
+    return old - sub == kQcSpots;
   }
 
   // A producer at the start of a queue chunk links the next one
   // (QueueChunk_impl.cuh:144-158).  A link needs its predecessor, so linking
   // is a chain; when producers already hold positions several queue chunks
-  // ahead (a burst), the chain is built up to 8 chunks at a time and offered
-  // in one CAS.  A lone producer is never further than one chunk ahead, so it
-  // links exactly one chunk, as the reference does.
-  __device__ static void preallocate(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos) {
+  // ahead (a burst), the group links up to one chunk per lane at once: one
+  // allocation for all, headers and links written in parallel, one CAS to
+  // attach the chain.  A lone producer is never more than one chunk ahead, so
+  // it links exactly one chunk, as the reference does.  c holds the range
+  // starting at pos.  Collective over g.
+  __device__ static void preallocate(HeapCore* h, ClassState* q, const Group& g, uint32_t c, uint32_t pos) {
+#ifdef OURO_SCAN_STATS
+    const long long t0 = clock64();
+#endif
     uint32_t* link = &h->meta[c].next;
-    if (ld_relaxed(link) != kEmpty) return;
-    const uint32_t back = ld_relaxed(&q->back.v);
-    uint32_t ahead = static_cast<int32_t>(back - pos) > static_cast<int32_t>(2u * kQcSpots)
-                         ? (back - pos) / kQcSpots - 1u : 1u;
-    if (ahead > 8u) ahead = 8u;
-    const uint32_t first = new_queue_chunk(h, q->inst, pos + kQcSpots);
-    if (first == kEmpty) return;
-    uint32_t last = first;
-    for (uint32_t i = 1; i < ahead; ++i) {
-      uint32_t nq = new_queue_chunk(h, q->inst, pos + (i + 1u) * kQcSpots);
-      if (nq == kEmpty) break;
-      st_relaxed(&h->meta[last].next, nq);
-      last = nq;
+    uint32_t ahead = 0;
+    if (g.is_leader() && ld_relaxed(link) == kEmpty) {
+      const uint32_t back = ld_relaxed(&q->back.v);
+      ahead = static_cast<int32_t>(back - pos) > static_cast<int32_t>(2u * kQcSpots)
+                  ? (back - pos) / kQcSpots - 1u : 1u;
+      if (ahead > static_cast<uint32_t>(g.size)) ahead = static_cast<uint32_t>(g.size);
     }
-    __threadfence();
-    if (atomicCAS(link, kEmpty, first) == kEmpty) {
-      for (uint32_t cc = first, i = 0; i < 8u; ++i) {
-        remember(h, q, cc, pos + (i + 1u) * kQcSpots);
-        if (cc == last) break;
-        cc = ld_relaxed(&h->meta[cc].next);
-      }
-    } else {
-      for (uint32_t cc = first, i = 0; i < 8u; ++i) {
-        uint32_t nx = ld_relaxed(&h->meta[cc].next);
-        reuse_put(h, &h->reuse[0], cc);
-        if (cc == last) break;
-        cc = nx;
-      }
+    ahead = bcast(g, ahead);
+    if (!ahead) return;
+    const uint32_t r = static_cast<uint32_t>(g.rank);
+    uint32_t mine = kEmpty;
+    const uint32_t got = alloc_chunks(h, g, ahead, q->inst, true, &mine);
+    const bool have = r < got && mine != kEmpty;
+    const uint32_t miss = __ballot_sync(g.mask, !have);
+    const uint32_t L = miss ? first_rank(g, miss) : static_cast<uint32_t>(g.size);
+    const uint32_t succ = __shfl_sync(g.mask, mine, lane_of_rank(g.mask, r + 1u < static_cast<uint32_t>(g.size)
+                                                                            ? static_cast<int>(r) + 1 : static_cast<int>(r)));
+    if (r < L) {
+      init_queue_chunk(h, mine, pos + (r + 1u) * kQcSpots, queue_tag(q));
+      if (r + 1u < L) st_relaxed(&h->meta[mine].next, succ);
+      __threadfence();
+    } else if (have) {
+      reuse_put(h, &h->reuse[0], mine);
     }
+    __syncwarp(g.mask);
+    if (L == 0u) return;
+    const uint32_t first = __shfl_sync(g.mask, mine, g.leader);
+    uint32_t ok = 0;
+    if (g.is_leader()) ok = atomicCAS(link, kEmpty, first) == kEmpty ? 1u : 0u;
+    ok = bcast(g, ok);
+    if (r < L) {
+      if (ok) remember(h, q, mine, pos + (r + 1u) * kQcSpots);
+      else reuse_put(h, &h->reuse[0], mine);
+    }
+#ifdef OURO_SCAN_STATS
+    if (g.is_leader()) {
+      atomicAdd(&h->scan[10].v, 1ull);
+      atomicAdd(&h->scan[11].v, static_cast<unsigned long long>(clock64() - t0));
+    }
+#endif
   }
 
   __device__ static Group half_of(const Group& g, uint32_t pos, uint32_t first) {
@@ -560,7 +690,7 @@ struct VlStore {
       if (g.is_leader()) set_status(h, kErrCorrupt);
       return;
     }
-    if (b % kQcSpots == 0u && g.is_leader()) preallocate(h, q, c1, b);
+    if (b % kQcSpots == 0u) preallocate(h, q, g, c1, b);
     // A range may cover several queue chunks (a group that grew many chunks
     // of a small class): walk the chain one segment per queue chunk.
     uint32_t qc = c1;
@@ -568,12 +698,10 @@ struct VlStore {
       const uint32_t room = kQcSpots - ((b + j0) % kQcSpots);
       j1 = E - j0 < room ? E : j0 + room;
       if (j0) {
-        if (g.is_leader()) {
-          qc = next_of(h, qc);
-          if (qc != kEmpty) preallocate(h, q, qc, b + j0);   // b + j0 starts a queue chunk
-        }
+        if (g.is_leader()) qc = next_of(h, qc);
         qc = bcast(g, qc);
         if (qc == kEmpty) break;
+        preallocate(h, q, g, qc, b + j0);   // b + j0 starts a queue chunk
       }
       const uint32_t r2 = (j1 - j0 + n - 1u) / n;
       for (uint32_t i = 0; i < r2; ++i) {
@@ -584,7 +712,9 @@ struct VlStore {
       }
       __syncwarp(g.mask);
       __threadfence();
-      if (g.is_leader()) count_enqueued(h, q, qc, j1 - j0);
+      uint32_t drained = 0;
+      if (g.is_leader()) drained = count_enqueued(h, q, qc, j1 - j0) ? 1u : 0u;
+      if (bcast(g, drained)) on_empty(h, q, g);
     }
   }
 
@@ -603,13 +733,15 @@ struct VlStore {
       if (sg.is_leader()) qc = next_of(h, c1);
       qc = bcast(sg, qc);
     }
-    if (qc != kEmpty) {
-      if (pos % kQcSpots == 0u) preallocate(h, q, qc, pos);
-      st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), v);
-    }
+    if (qc == kEmpty) return;
+    const uint32_t starts = __ballot_sync(sg.mask, pos % kQcSpots == 0u);
+    if (starts) preallocate(h, q, sg, qc, __shfl_sync(sg.mask, pos, __ffs(starts) - 1));
+    st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), v);
     __syncwarp(sg.mask);
     __threadfence();
-    if (sg.is_leader() && qc != kEmpty) count_enqueued(h, q, qc, static_cast<uint32_t>(sg.size));
+    uint32_t drained = 0;
+    if (sg.is_leader()) drained = count_enqueued(h, q, qc, static_cast<uint32_t>(sg.size)) ? 1u : 0u;
+    if (bcast(sg, drained)) on_empty(h, q, sg);
   }
 
   __device__ static uint32_t consume_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos) {
@@ -627,10 +759,12 @@ struct VlStore {
       if (sg.is_leader()) qc = next_of(h, c1);
       qc = bcast(sg, qc);
     }
-    uint32_t v = kEmpty;
-    if (qc != kEmpty) v = take_slot(h, queue_slots(h, qc) + (pos % kQcSpots));
+    if (qc == kEmpty) return kEmpty;
+    const uint32_t v = take_slot(h, queue_slots(h, qc) + (pos % kQcSpots));
     __syncwarp(sg.mask);
-    if (sg.is_leader() && qc != kEmpty) count_removed(h, q, qc, static_cast<uint32_t>(sg.size));
+    uint32_t drained = 0;
+    if (sg.is_leader()) drained = count_removed(h, q, qc, static_cast<uint32_t>(sg.size)) ? 1u : 0u;
+    if (bcast(sg, drained)) on_empty(h, q, sg);
     return v;
   }
 
@@ -639,19 +773,26 @@ struct VlStore {
     uint32_t b = atomicAdd(&q->back.v, 1u);
     uint32_t qc = locate_live(h, q, ld_acquire(&q->back_ptr), b);
     if (qc == kEmpty || qc == kBehind) { set_status(h, kErrCorrupt); return false; }
-    if (b % kQcSpots == 0u) preallocate(h, q, qc, b);
+    const Group self = make_group(1u << lane_id());
+    if (b % kQcSpots == 0u) preallocate(h, q, self, qc, b);
     st_relaxed(qpos, b);
     __threadfence();
     st_release(queue_slots(h, qc) + (b % kQcSpots), c);
     __threadfence();
-    count_enqueued(h, q, qc, 1u);
+    if (count_enqueued(h, q, qc, 1u)) on_empty(h, q, self);
     return true;
   }
   struct Cursor { uint32_t chunk; };
   __device__ static Cursor cursor(ClassState* q) { return Cursor{ld_acquire(&q->front_ptr)}; }
   __device__ static uint32_t peek(HeapCore* h, ClassState* q, uint32_t pos, Cursor& cur) {
     uint32_t qc = recall(h, q, pos);
-    if (qc == kEmpty) qc = locate(h, cur.chunk, pos);
+    if (qc == kEmpty) {
+      // walk from the cursor's chunk, or from front_ptr once the cursor's chunk fell behind it
+      const uint32_t fp = ld_acquire(&q->front_ptr);
+      const uint32_t fr = ld_relaxed(&h->meta[fp].vstart) / kQcSpots;
+      const uint32_t cr = ld_relaxed(&h->meta[cur.chunk].vstart) / kQcSpots;
+      qc = locate(h, static_cast<int32_t>(cr - fr) < 0 ? fp : cur.chunk, pos);
+    }
     if (qc == kBehind) {
       cur.chunk = ld_acquire(&q->front_ptr);
       return kTomb;
@@ -665,12 +806,12 @@ struct VlStore {
     if (qc == kEmpty || qc == kBehind) return;
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
     __threadfence();
-    count_removed(h, q, qc, 1u);
+    if (count_removed(h, q, qc, 1u)) on_empty(h, q, make_group(1u << lane_id()));
   }
   // Front moves over removed entries.  The leader walks the chain: per round
   // the group's positions span at most two queue chunks (4 x 32 < 2048), the
   // current one and its successor.  Drained queue chunks leave the chain
-  // through count_removed / set_front, not here.
+  // through count_removed / on_empty, not here.
   __device__ static void advance_front(HeapCore* h, ClassState* q, const Group& g) {
     uint32_t f = 0, back = 0, qc = kEmpty, from = 0;
     if (g.is_leader()) {
