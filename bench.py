@@ -150,6 +150,10 @@ class OursArm:
     def flags(self):
         return self.heap.status()["flags"]
 
+    def detail(self) -> str:
+        st = self.heap.status()
+        return f"timeouts {st['timeouts']} at wait sites {st['timeout_sites']:#x}, nulls {st['null_results']}"
+
 
 class ReferenceArm:
     name = "reference"
@@ -250,8 +254,9 @@ def run_cells(arm, cells, n, block, stream, ptrs, counters, flush, steps, warmup
             if rep == 0:
                 flags = arm.flags()
                 if flags & ~1:
+                    why = arm.detail() if hasattr(arm, "detail") else ""
                     arm.close()
-                    raise BenchAbort(f"device error flags {flags} after {v}:{size}")
+                    raise BenchAbort(f"device error flags {flags} after {v}:{size} (first repetition) {why}")
         e2e_ms = None
         if e2e:
             sizes_h.fill_(size)
@@ -265,9 +270,10 @@ def run_cells(arm, cells, n, block, stream, ptrs, counters, flush, steps, warmup
             stream.synchronize()
             e2e_ms = ev[0].elapsed_time(ev[1])
         flags = arm.flags()
+        why = arm.detail() if hasattr(arm, "detail") and flags & ~1 else ""
         arm.close()
         if flags & ~1:
-            raise BenchAbort(f"device error flags {flags} after {v}:{size}")
+            raise BenchAbort(f"device error flags {flags} after {v}:{size} {why}")
         res[(v, size)] = (a_ms, f_ms, e2e_ms)
         print(f"[bench] {tag} {v}:{size} alloc {np.mean(a_ms):.4f} ms free {np.mean(f_ms):.4f} ms "
               f"({time.perf_counter() - t0:.2f}s)", file=sys.stderr, flush=True)
@@ -310,6 +316,67 @@ def cpu_baseline(cells, n, heap_bytes) -> dict:
                               "sample": f"glibc malloc/free, {len(HEADLINE_SIZES)} sizes x {n} requests "
                                         f"(the same requests for every instantiation)"}
     return out
+
+
+# Hot-line RMWs per warp group that every group of a class serialises on: the
+# class semaphore plus the front ticket (page alloc), back ticket (page free) or
+# scan cursor (chunk alloc); chunk free only signals the semaphore.
+HOT_RMW = {("page", "alloc"): 2, ("page", "free"): 2, ("chunk", "alloc"): 2, ("chunk", "free"): 1}
+# Per-lane L2 atomics per alloc+free pair of the reference's algorithm (g = 32 lanes per group).
+REF_ATOMICS_PER_PAIR = {"P": 2 + 4 / 32, "VAP": 4 + 4 / 32, "VLP": 4 + 4 / 32,
+                        "C": 4 + 2 / 32, "VAC": 4 + 2 / 32, "VLC": 4 + 2 / 32}
+
+
+def roofline(res, n, steps) -> dict:
+    """Roofline of the dominant kernel: the (kernel, instantiation) pair with the
+    largest share of the timed kernel time.  Every warp group of a class
+    serialises on the class's hot lines, so the bound is L2 atomic throughput
+    on those lines: achieved = hot RMWs per launch / average launch time,
+    against the measured single-address atomic rate times the number of
+    distinct hot lines (2, or 1 for chunk free)."""
+    import ouroboros_b200 as ob
+    per = {}
+    for (v, size), (a, f, _) in res.items():
+        for kern, ms in (("alloc", a), ("free", f)):
+            t = per.setdefault((v, kern), [0.0, 0])
+            t[0] += float(np.sum(ms))
+            t[1] += len(ms)
+    total = sum(t[0] for t in per.values())
+    (v, kern), (ms_sum, launches) = max(per.items(), key=lambda kv: kv[1][0])
+    avg_ms = ms_sum / launches
+    kind = "page" if v in ("P", "VAP", "VLP") else "chunk"
+    hot_lines = HOT_RMW[(kind, kern)]
+    groups = n / 32.0
+    achieved = hot_lines * groups / (avg_ms * 1e-3) / 1e9
+    hot = ob.measure_atomics(1)
+    distinct = ob.measure_atomics(0)
+    peak = hot_lines * hot
+    vidx = VARIANTS.index(v)
+    traffic = None
+    try:
+        traffic = json.load(open(TRAFFIC_FILE)).get(f"k_{kern}<{vidx}>")
+    except Exception:
+        pass
+    peaks = measured_peaks()
+    ref_atomics = REF_ATOMICS_PER_PAIR[v] / 2.0 * n
+    return {
+        "bound": "l2_atomic", "kernel": f"k_{kern}<{vidx}> ({v})", "share": round(ms_sum / total, 4),
+        "achieved": round(achieved, 4), "peak": round(peak, 4), "unit": "G hot-line RMW/s",
+        "frac": round(achieved / peak, 4), "traffic": traffic,
+        "traffic_unit": "bytes per launch (dram read + write, ncu)",
+        "peak_source": f"measured live by ouro_measure_atomics: one hot 32-bit address, one RMW per warp, "
+                       f"x{hot_lines} independent hot lines",
+        "avg_launch_ms": round(avg_ms, 5), "launches": launches,
+        "reference_model": {
+            "what": "per-lane L2 atomics of the reference's algorithm for this launch (half of an alloc+free pair)",
+            "atomics_per_launch": ref_atomics,
+            "achieved_gops": round(ref_atomics / (avg_ms * 1e-3) / 1e9, 3),
+            "peak_gops": round(distinct, 2), "peak_source": "measured live: distinct-address atomics, all SMs",
+            "frac": round(ref_atomics / (avg_ms * 1e-3) / 1e9 / distinct, 5)},
+        "hbm": {"bytes_per_launch": 16.0 * n, "achieved_gbs": round(16.0 * n / (avg_ms * 1e-3) / 1e9, 2),
+                "peak_gbs": peaks.get("hbm_gbs"), "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                "note": "per request 8 B pointer + 4 B entry read + 4 B entry write"},
+    }
 
 
 def measured_peaks() -> dict:
@@ -437,33 +504,7 @@ def main():
                           "h2d_bytes_per_step": 4 * n * len(cells), "d2h_bytes_per_step": 8 * n * len(cells),
                           "what": "per cell: request sizes host->device (pinned), alloc launch, pointer array "
                                   "device->host, free launch, through the C ABI; after the timed repetitions"}
-        # roofline of the dominant kernel: the hot counters of a size class
-        import ouroboros_b200 as ob
-        hot = ob.measure_atomics(1)
-        distinct = ob.measure_atomics(0)
-        dom = "alloc" if alloc_ms >= free_ms else "free"
-        dom_ms = (alloc_ms if dom == "alloc" else free_ms) / (len(cells) * args.steps)
-        # per launch: every warp group issues one atomic on each of two counter
-        # lines (alloc: semaphore + front, free: back + semaphore)
-        requests = 2.0 * n / 32.0
-        achieved = requests / (dom_ms * 1e-3) / 1e9
-        traffic = None
-        try:
-            traffic = json.load(open(TRAFFIC_FILE)).get(f"k_{dom}")
-        except Exception:
-            pass
-        peaks = measured_peaks()
-        hbm_bytes = 16.0 * n   # per op: 8 B pointer + 4 B slot read + 4 B slot write
-        out["roofline"] = {
-            "bound": "l2_atomic", "kernel": f"k_{dom}", "achieved": round(achieved, 4),
-            "peak": round(2 * hot, 4), "unit": "G hot-counter atomics/s", "frac": round(achieved / (2 * hot), 4),
-            "traffic": traffic,
-            "peak_source": "measured live: one hot 32-bit address, one atomicAdd per warp (x2 counter lines)",
-            "distinct_address_peak_gops": round(distinct, 2),
-            "hbm": {"achieved_gbs": round(hbm_bytes / (dom_ms * 1e-3) / 1e9, 2),
-                    "peak_gbs": peaks.get("hbm_gbs"), "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
-            "avg_launch_ms": round(dom_ms, 5),
-        }
+        out["roofline"] = roofline(res, n, args.steps)
         if not args.no_cpu and rank == 0:
             out["cpu_baseline"] = cpu_baseline(cells, n, heap_bytes)
     if rank == 0:

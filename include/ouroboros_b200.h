@@ -102,6 +102,12 @@ typedef struct {
   uint64_t timeouts;          /* bounded waits that gave up                 */
   uint64_t chunk_allocs;      /* chunk allocations (Statistics.h:11)        */
   uint64_t next_free_chunk;   /* Memory::next_free_chunk                    */
+  uint32_t timeout_sites;     /* one bit per kind of wait that gave up: 1 semaphore rounds,
+                                 2 semaphore CAS, 4 semaphore reservation, 8 queue slot still
+                                 full, 16 queue slot never written, 32 array index entry,
+                                 64 linked successor, 128 walk length, 256 walks meeting
+                                 recycled chunks, 512 / 1024 chunk reuse ring read / write,
+                                 2048 chunk-queue scan */
 } ouro_heap_status;
 /* Device-side status; clear != 0 resets flags and counters afterwards. */
 int ouro_get_status(ouro_heap* h, ouro_heap_status* out, int clear);
@@ -174,12 +180,14 @@ int ouro_check_heap(ouro_heap* h, ouro_heap_report* out);
  * in G operations per second. */
 int ouro_measure_atomics(int mode, double* gops);
 
-/* Diagnostic counters of the chunk-based allocation path, 12 words: groups,
- * probes, misses, next-fit runs; SM cycles summed over group leaders spent in
- * the semaphore, the scan, dequeues and page claims; groups slower than 2^20
- * cycles; the slowest group's cycles; front advances and the cycles inside
- * them.  All zero unless the library was built with -DOURO_SCAN_STATS.  No
- * counterpart in the reference. */
+/* Diagnostic counters, 12 words.  Chunk-based heaps: groups, probes, misses,
+ * next-fit runs; for groups slower than 2^19 SM cycles the cycles their
+ * leaders spent in the semaphore, the scan, dequeues and page claims; the
+ * number of such groups; the slowest group's cycles; their probes and misses.
+ * Page-based heaps: allocating groups, their cycles in the semaphore and in
+ * taking entries, -, freeing groups, their cycles, the slowest free, -,
+ * allocating groups slower than 2^20 cycles, the slowest allocation.  All zero unless the library
+ * was built with -DOURO_SCAN_STATS.  No counterpart in the reference. */
 int ouro_scan_stats(ouro_heap* h, uint64_t* out12, int clear);
 
 const char* ouro_status_string(int code);

@@ -53,7 +53,8 @@ class _Info(ctypes.Structure):
 
 class _Status(ctypes.Structure):
     _fields_ = [("flags", ctypes.c_uint32), ("null_results", ctypes.c_uint64), ("timeouts", ctypes.c_uint64),
-                ("chunk_allocs", ctypes.c_uint64), ("next_free_chunk", ctypes.c_uint64)]
+                ("chunk_allocs", ctypes.c_uint64), ("next_free_chunk", ctypes.c_uint64),
+                ("timeout_sites", ctypes.c_uint32)]
 
 
 class _AllocReport(ctypes.Structure):
@@ -210,8 +211,8 @@ class Ouroboros:
     def scan_stats(self, clear: bool = False) -> dict:
         out = np.zeros(12, dtype=np.uint64)
         _check(lib().ouro_scan_stats(self._handle(), out.ctypes.data, int(clear)), "ouro_scan_stats")
-        names = ("groups", "probes", "misses", "runs", "cyc_sem", "cyc_scan", "cyc_dequeue", "cyc_claim",
-                 "slow_groups", "cyc_max", "front_advances", "cyc_front")
+        names = ("groups", "probes", "misses", "runs", "slow_cyc_sem", "slow_cyc_scan", "slow_cyc_dequeue",
+                 "slow_cyc_claim", "slow_groups", "cyc_max", "slow_probes", "slow_misses")
         return {k: int(x) for k, x in zip(names, out)}
 
     def check_heap(self) -> dict:

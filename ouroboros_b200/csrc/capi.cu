@@ -310,8 +310,14 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
   core.base = h->base;
   core.alloc_bytes = L.alloc_bytes;
   core.heap_bytes = heap_bytes;
-  for (int i = 0; i < 2; ++i) core.reuse[i].ring = reinterpret_cast<uint32_t*>(h->base + L.reuse_off) + i * kReuseSize;
   const int kind = variant / 2;
+  if (kind != 0) {
+    // usable base chunks (index + 1 < max_chunks); every class starts with
+    // one queue chunk and keeps its margin
+    core.budget_limit = L.max_chunks - 1u;
+    core.budget.v = static_cast<unsigned long long>(kNumClasses) * (1u + queue_margin(kind));
+  }
+  for (int i = 0; i < 2; ++i) core.reuse[i].ring = reinterpret_cast<uint32_t*>(h->base + L.reuse_off) + i * kReuseSize;
   for (uint32_t c = 0; c < kNumClasses; ++c) {
     ClassState& q = core.cls[c];
     q.sem.v = SemWord::kInit;
@@ -485,6 +491,7 @@ int ouro_get_status(ouro_heap* h, ouro_heap_status* out, int clear) {
   out->timeouts = core.timeouts.v;
   out->chunk_allocs = core.chunk_allocs.v;
   out->next_free_chunk = core.next_free_chunk.v;
+  out->timeout_sites = core.timeout_sites.v;
   if (clear) {
     const size_t off = offsetof(HeapCore, status);
     const size_t len = offsetof(HeapCore, chunk_allocs) - off;

@@ -36,8 +36,11 @@ constexpr uint32_t kInstalling = 0xFFFFFFFCu;  // queue-chunk link being install
 // pre-allocated installs one itself (the pre-allocation failed for lack of
 // chunks, or its lane is slow).
 constexpr uint32_t kInstallAfter = 256u;
-// Pooled chunks kept for queue chunks once the heap has no fresh chunk left.
-constexpr uint32_t kQueueChunkReserve = 2u * kNumClasses;
+// Queue chunks per class, beyond those holding its entries, that the chunk
+// budget of the virtualized queues keeps free: partial chunks at both ends
+// of the window, the pre-allocated successor, one more for a front that
+// recycles late, and for linked queues the hold-back of drained chunks.
+__host__ __device__ constexpr uint32_t queue_margin(int kind) { return kind == 1 ? 4u : kind == 2 ? 4u + kOldHold : 0u; }
 // Slots of the linked queues' chunk index (recently linked queue chunks).
 constexpr uint32_t kSkipSlots = 1024u;
 

@@ -45,6 +45,7 @@ struct alignas(128) ClassState {
   uint32_t cls, inst, page_size, page_shift, ppc, words;
   uint32_t front_ptr, back_ptr, old_ptr, old_count;  // linked: chunk indices
   uint32_t class_pages;           // pages ever created for the class (queue capacity guard)
+  uint32_t class_chunks;          // chunk-based: chunks ever created for the class (budget)
   uint32_t page_cap;
   uint32_t clean_on_recycle;      // chunk queues: queue chunks hold kTomb entries when drained
   uint32_t* skip;                 // linked: index of recently linked queue chunks
@@ -70,18 +71,19 @@ struct alignas(128) HeapCore {
   char* base;
   unsigned long long alloc_bytes;
   unsigned long long heap_bytes;
+  unsigned long long budget_limit;     // virtualized: chunks the budget may commit (0: no budget)
   // hot / warm counters
   Line<unsigned long long> next_free_chunk;
   Line<uint32_t> status;
   Line<unsigned long long> oom;        // null results handed out
   Line<unsigned long long> timeouts;   // bounded waits that gave up
+  Line<uint32_t> timeout_sites;        // WaitSite bits of the waits that gave up
   Line<unsigned long long> chunk_allocs;
+  Line<unsigned long long> budget;     // virtualized: data chunks + queue chunks the classes need
   ReuseQueue reuse[2];
   ClassState cls[kNumClasses];
-  // chunk-based path counters, only written when built with OURO_SCAN_STATS:
-  // groups, probes, misses, next-fit runs; leader cycles in semaphore, scan,
-  // dequeue, claim; groups slower than 2^20 cycles, slowest group's cycles,
-  // front advances, cycles inside front advances
+  // diagnostic counters, only written when built with OURO_SCAN_STATS (their
+  // meaning per heap kind is listed at ouro_scan_stats in the C header)
   Line<unsigned long long> scan[kScanCounters];
 };
 
@@ -89,8 +91,25 @@ constexpr size_t kCoreBytes = 16384;
 static_assert(sizeof(HeapCore) <= kCoreBytes, "control block grew past its region");
 
 __device__ __forceinline__ void set_status(HeapCore* h, uint32_t bits) { atomicOr(&h->status.v, bits); }
-__device__ __forceinline__ void note_timeout(HeapCore* h) {
+// Bounded waits, one bit each in HeapCore::timeout_sites when they give up.
+enum WaitSite : uint32_t {
+  kWaitSemRounds = 1u << 0,    // semaphore: rounds of a group's acquisition
+  kWaitSemCas = 1u << 1,       // semaphore: CAS retries
+  kWaitSemReserve = 1u << 2,   // semaphore: reserved pages that do not arrive
+  kWaitSlotEmpty = 1u << 3,    // queue slot still holding the previous lap's entry
+  kWaitSlotFull = 1u << 4,     // queue slot whose producer does not write it
+  kWaitIndexEntry = 1u << 5,   // virtualized array: queue chunk of a range
+  kWaitLink = 1u << 6,         // linked: successor of a queue chunk
+  kWaitLocateHops = 1u << 7,   // linked: walk longer than 2^20 hops
+  kWaitLocateStale = 1u << 8,  // linked: walks kept meeting recycled chunks
+  kWaitReuseRead = 1u << 9,    // chunk reuse ring: reserved entry not written
+  kWaitReusePut = 1u << 10,    // chunk reuse ring: slot not yet read
+  kWaitChunkScan = 1u << 11,   // chunk queue: scan for a chunk with free pages
+};
+
+__device__ __forceinline__ void note_timeout(HeapCore* h, uint32_t site) {
   set_status(h, kErrTimeout);
+  atomicOr(&h->timeout_sites.v, site);
   atomicAdd(&h->timeouts.v, 1ull);
 }
 
@@ -140,9 +159,8 @@ __host__ inline bool compute_layout(int kind, unsigned long long heap_bytes, Lay
 // ------------------------------------------------------- reuse queue
 // The chunk reuse ring (queues/Queue_impl.cuh:20-66): FIFO of whole chunks
 // that left a queue.  take() serves up to k chunks for one group.
-__device__ inline uint32_t reuse_take(HeapCore* h, ReuseQueue* r, uint32_t k, uint32_t* first_pos,
-                                      int32_t floor = 0) {
-  int32_t old = atomicSub(&r->count.v, static_cast<int32_t>(k)) - floor;
+__device__ inline uint32_t reuse_take(HeapCore* h, ReuseQueue* r, uint32_t k, uint32_t* first_pos) {
+  int32_t old = atomicSub(&r->count.v, static_cast<int32_t>(k));
   uint32_t got = old <= 0 ? 0u : (static_cast<uint32_t>(old) < k ? static_cast<uint32_t>(old) : k);
   if (got < k) atomicAdd(&r->count.v, static_cast<int32_t>(k - got));
   if (got) *first_pos = atomicAdd(&r->front.v, got);
@@ -153,7 +171,7 @@ __device__ inline uint32_t reuse_read(HeapCore* h, ReuseQueue* r, uint32_t pos) 
   uint32_t* s = r->ring + (pos & (kReuseSize - 1u));
   uint32_t v, it = 0;
   while ((v = ld_acquire(s)) == kEmpty) {
-    if (it >= kSpinLimit) { note_timeout(h); return kEmpty; }
+    if (it >= kSpinLimit) { note_timeout(h, kWaitReuseRead); return kEmpty; }
     backoff(it);
   }
   st_relaxed(s, kEmpty);
@@ -175,7 +193,7 @@ __device__ inline void reuse_put(HeapCore* h, ReuseQueue* r, uint32_t chunk) {
   uint32_t* s = r->ring + (pos & (kReuseSize - 1u));
   uint32_t it = 0;
   while (ld_relaxed(s) != kEmpty) {
-    if (it >= kSpinLimit) { note_timeout(h); return; }
+    if (it >= kSpinLimit) { note_timeout(h, kWaitReusePut); return; }
     backoff(it);
   }
   st_release(s, chunk);
@@ -193,14 +211,7 @@ __device__ inline uint32_t alloc_chunks(HeapCore* h, const Group& g, uint32_t k,
   uint32_t from_reuse = 0, rpos = 0;
   unsigned long long first = 0;
   if (g.is_leader()) {
-    // Once the bump pointer is spent, the last few pooled chunks are kept for
-    // queue chunks: a virtualized queue that cannot grow would strand the
-    // pages already promised to it.  (Never reached below capacity, so the
-    // reuse-first order of the reference is unchanged there.)
-    int32_t floor = 0;
-    if (!queue_chunk && r == &h->reuse[0] && ld_relaxed(&h->next_free_chunk.v) + factor >= h->max_chunks)
-      floor = static_cast<int32_t>(kQueueChunkReserve);
-    from_reuse = reuse_take(h, r, k, &rpos, floor);
+    from_reuse = reuse_take(h, r, k, &rpos);
     if (from_reuse < k) first = atomicAdd(&h->next_free_chunk.v, (unsigned long long)(k - from_reuse) * factor);
     atomicAdd(&h->chunk_allocs.v, (unsigned long long)k);
   }

@@ -45,15 +45,37 @@ __device__ __forceinline__ void init_data_chunk(HeapCore* h, ClassState* q, uint
 }
 
 // Queue capacity guard: a class may not own more pages than its queue holds
-// (the reference traps in that case, PageQueue_impl.cuh:34).
-__device__ __forceinline__ bool reserve_class_pages(HeapCore* h, ClassState* q, uint32_t pages) {
+// (the reference traps in that case, PageQueue_impl.cuh:34).  Returns the
+// class's page count before the reservation, kEmpty when refused.
+__device__ __forceinline__ uint32_t reserve_class_pages(HeapCore* h, ClassState* q, uint32_t pages) {
   uint32_t old = atomicAdd(&q->class_pages, pages);
   if (old + pages > q->page_cap || old + pages < old) {
     atomicSub(&q->class_pages, pages);
     set_status(h, kErrQueueFull);
-    return false;
+    return kEmpty;
   }
-  return true;
+  return old;
+}
+
+// Virtualized queues take their queue chunks from the same pool as data
+// chunks.  A class only grows while the queue chunks it will need at its new
+// size still fit: `budget` counts data chunks plus, per class, the queue
+// chunks for its entries and a margin, against the usable chunks.  Without
+// it the last data chunks would leave no queue chunk for the entries they
+// bring, and producers would wait for a link that cannot come.  The queue of
+// the class grows from e0 entries by `per` entries per chunk; returns how
+// many of the k chunks (factor base chunks each) the class may add.
+__device__ __forceinline__ uint32_t queue_chunks_for(uint32_t entries) { return (entries + kQcSpots - 1u) / kQcSpots; }
+
+__device__ inline uint32_t commit_budget(HeapCore* h, uint32_t k, uint32_t factor, uint32_t e0, uint32_t per) {
+  for (uint32_t kk = k; kk; kk >>= 1) {
+    const unsigned long long d = static_cast<unsigned long long>(kk) * factor + queue_chunks_for(e0 + kk * per) -
+                                 queue_chunks_for(e0);
+    const unsigned long long old = atomicAdd(&h->budget.v, d);
+    if (old + d <= h->budget_limit) return kk;
+    atomicAdd(&h->budget.v, 0ull - d);
+  }
+  return 0u;
 }
 
 // ============================================================ page queues
@@ -63,14 +85,25 @@ __device__ __forceinline__ bool reserve_class_pages(HeapCore* h, ClassState* q, 
 // the back with one position reservation, and credit the semaphore.
 template <class Store>
 __device__ uint32_t page_grow(HeapCore* h, ClassState* q, const Group& g, uint32_t k) {
-  uint32_t ok = 1u;
-  if (g.is_leader()) ok = reserve_class_pages(h, q, k * q->ppc) ? 1u : 0u;
-  ok = bcast(g, ok);
+  const uint32_t factor = instance_factor(q->inst);
+  uint32_t kk = 0;   // chunks this group may add
+  if (g.is_leader()) {
+    const uint32_t old = reserve_class_pages(h, q, k * q->ppc);
+    if (old != kEmpty) {
+      kk = k;
+      if constexpr (Store::kKind != 0) kk = commit_budget(h, k, factor, old, q->ppc);
+      if (kk < k) atomicSub(&q->class_pages, (k - kk) * q->ppc);
+    }
+  }
+  kk = bcast(g, kk);
   uint32_t got = 0, c = kEmpty;
-  if (ok) {
-    got = alloc_chunks(h, g, k, q->inst, false, &c);
+  if (kk) {
+    got = alloc_chunks(h, g, kk, q->inst, false, &c);
     if (static_cast<uint32_t>(g.rank) < got && c != kEmpty) init_data_chunk(h, q, c, false);
-    if (g.is_leader() && got < k) atomicSub(&q->class_pages, (k - got) * q->ppc);
+    if (g.is_leader() && got < kk) {
+      atomicSub(&q->class_pages, (kk - got) * q->ppc);
+      if constexpr (Store::kKind != 0) atomicAdd(&h->budget.v, 0ull - static_cast<unsigned long long>(kk - got) * factor);
+    }
   }
   const uint32_t E = got * q->ppc;
   if (E) {
@@ -188,18 +221,12 @@ __device__ void help_front(HeapCore* h, ClassState* q, const Group& g) {
   uint32_t mine = 0;
   if (g.is_leader()) mine = atomicCAS(&q->advancing.v, 0u, 1u) == 0u ? 1u : 0u;
   if (!bcast(g, mine)) return;
-#ifdef OURO_SCAN_STATS
-  const long long t0 = clock64();
-#endif
   Store::advance_front(h, q, g);
   __syncwarp(g.mask);
   if (g.is_leader()) {
     __threadfence();
     atomicExch(&q->advancing.v, 0u);
-#ifdef OURO_SCAN_STATS
-    atomicAdd(&h->scan[10].v, 1ull);
-    atomicAdd(&h->scan[11].v, static_cast<unsigned long long>(clock64() - t0));
-#endif
+
   }
 }
 
@@ -298,8 +325,26 @@ __device__ void claim_pages(HeapCore* h, const Group& s, uint32_t c, uint32_t go
 // queue entry, then credit the semaphore.
 template <class Store>
 __device__ uint32_t chunk_grow(HeapCore* h, ClassState* q, const Group& g, uint32_t k) {
+  const uint32_t factor = instance_factor(q->inst);
+  uint32_t kk = k;
+  if constexpr (Store::kKind != 0) {
+    // a chunk has at most one live entry; removed entries wait for the front:
+    // the budget counts two queue entries per chunk
+    if (g.is_leader()) {
+      const uint32_t old = atomicAdd(&q->class_chunks, k);
+      kk = commit_budget(h, k, factor, 2u * old, 2u);
+      if (kk < k) atomicSub(&q->class_chunks, k - kk);
+    }
+    kk = bcast(g, kk);
+  }
   uint32_t c = kEmpty;
-  uint32_t got = alloc_chunks(h, g, k, q->inst, false, &c);
+  uint32_t got = kk ? alloc_chunks(h, g, kk, q->inst, false, &c) : 0u;
+  if constexpr (Store::kKind != 0) {
+    if (g.is_leader() && got < kk) {
+      atomicSub(&q->class_chunks, kk - got);
+      atomicAdd(&h->budget.v, 0ull - static_cast<unsigned long long>(kk - got) * factor);
+    }
+  }
   const bool mine = static_cast<uint32_t>(g.rank) < got && c != kEmpty;
   if (mine) {
     init_data_chunk(h, q, c, true);
@@ -373,7 +418,7 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
     uint32_t c = kEmpty, got = 0, last = 0, help = 0;
     if (s.is_leader()) {
       if (iter > 4u * kSpinLimit) {
-        note_timeout(h);
+        note_timeout(h, kWaitChunkScan);
         c = kTomb;
       } else {
         if (pos == run_end) {
@@ -442,12 +487,16 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
     atomicAdd(&h->scan[1].v, st_probe);
     atomicAdd(&h->scan[2].v, st_miss);
     atomicAdd(&h->scan[3].v, st_run);
-    atomicAdd(&h->scan[4].v, static_cast<unsigned long long>(t_sem));
-    atomicAdd(&h->scan[5].v, static_cast<unsigned long long>(clock64() - t_begin - t_sem - t_claim - t_deq));
-    atomicAdd(&h->scan[6].v, static_cast<unsigned long long>(t_deq));
-    atomicAdd(&h->scan[7].v, static_cast<unsigned long long>(t_claim));
     const unsigned long long total = static_cast<unsigned long long>(clock64() - t_begin);
-    if (total > (1ull << 20)) atomicAdd(&h->scan[8].v, 1ull);
+    if (total > (1ull << 19)) {   // slow groups: where their time went
+      atomicAdd(&h->scan[4].v, static_cast<unsigned long long>(t_sem));
+      atomicAdd(&h->scan[5].v, static_cast<unsigned long long>(clock64() - t_begin - t_sem - t_claim - t_deq));
+      atomicAdd(&h->scan[6].v, static_cast<unsigned long long>(t_deq));
+      atomicAdd(&h->scan[7].v, static_cast<unsigned long long>(t_claim));
+      atomicAdd(&h->scan[8].v, 1ull);
+      atomicAdd(&h->scan[10].v, st_probe);
+      atomicAdd(&h->scan[11].v, st_miss);
+    }
     atomicMax(&h->scan[9].v, total);
   }
 #endif

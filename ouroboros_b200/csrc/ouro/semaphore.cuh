@@ -80,7 +80,7 @@ __device__ inline uint32_t sem_acquire(HeapCore* h, ClassState* q, const Group& 
     uint32_t mode = kFail, arg = 0;
     if (g.is_leader()) {
       if (round > kSpinLimit) {
-        note_timeout(h);
+        note_timeout(h, kWaitSemRounds);
         mode = kFail;
       } else {
         // fast path: one subtract (optimistic on the first round)
@@ -134,7 +134,7 @@ __device__ inline uint32_t sem_acquire(HeapCore* h, ClassState* q, const Group& 
             }
             unsigned long long seen = atomicCAS(&q->sem.v, v, nv);
             if (seen == v) break;
-            if (tries > kSpinLimit) { note_timeout(h); mode = kFail; break; }
+            if (tries > kSpinLimit) { note_timeout(h, kWaitSemCas); mode = kFail; break; }
             // contended: back off before re-reading, so that thousands of
             // arriving warps do not turn the word into a CAS storm
             __nanosleep(16u << (tries < 6u ? tries : 6u));
@@ -148,7 +148,7 @@ __device__ inline uint32_t sem_acquire(HeapCore* h, ClassState* q, const Group& 
               long long c = SemWord::count(w);
               long long cover = c + static_cast<long long>(SemWord::exp_chunks(w)) * ppc;
               if (c >= static_cast<long long>(n) || static_cast<long long>(SemWord::reserved(w)) >= cover) break;
-              if (it >= kSpinLimit) { note_timeout(h); break; }
+              if (it >= kSpinLimit) { note_timeout(h, kWaitSemReserve); break; }
               backoff(it);
             }
             atomicAdd(&q->sem.v, SemWord::sub(0) - (static_cast<unsigned long long>(n) << SemWord::kResShift));

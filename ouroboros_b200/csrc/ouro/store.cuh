@@ -27,7 +27,7 @@ __device__ __forceinline__ int lane_of_rank(uint32_t mask, int r) {
 __device__ __forceinline__ bool wait_slot_empty(HeapCore* h, uint32_t* s) {
   uint32_t it = 0;
   while (ld_relaxed(s) != kEmpty) {
-    if (it >= kSpinLimit) { note_timeout(h); return false; }
+    if (it >= kSpinLimit) { note_timeout(h, kWaitSlotEmpty); return false; }
     backoff(it);
   }
   return true;
@@ -37,7 +37,7 @@ __device__ __forceinline__ bool wait_slot_empty(HeapCore* h, uint32_t* s) {
 __device__ __forceinline__ uint32_t take_slot(HeapCore* h, uint32_t* s) {
   uint32_t v, it = 0;
   while ((v = ld_acquire(s)) == kEmpty) {
-    if (it >= kSpinLimit) { note_timeout(h); return kEmpty; }
+    if (it >= kSpinLimit) { note_timeout(h, kWaitSlotFull); return kEmpty; }
     backoff(it);
   }
   st_relaxed(s, kEmpty);
@@ -176,7 +176,7 @@ struct VaStore {
     uint32_t* e = q->ring + vid(pos);
     uint32_t c, it = 0;
     while ((c = ld_acquire(e)) == kEmpty || c == kInstalling) {
-      if (it >= kSpinLimit) { note_timeout(h); return kEmpty; }
+      if (it >= kSpinLimit) { note_timeout(h, kWaitIndexEntry); return kEmpty; }
       if (c == kEmpty && it >= kInstallAfter && (it & 63u) == 0u)
         install_queue_chunk(h, e, q->inst, pos - pos % kQcSpots, queue_tag(q));
       backoff(it);
@@ -369,6 +369,8 @@ struct VaStore {
 struct VlStore {
   static constexpr int kKind = 2;
   static constexpr uint32_t kBehind = 0xFFFFFFFDu;
+  static constexpr uint32_t kStale = 0xFFFFFFFBu;   // a walk met a recycled chunk
+  static constexpr uint32_t kRecallPolls = 48u;            // index polls before walking the chain
 
   // Direct-mapped index of recently linked queue chunks (virtual chunk id mod
   // kSkipSlots).  An entry is only a hint, valid while the chunk carries the
@@ -389,33 +391,51 @@ struct VlStore {
   }
 
   // Walk from `from` to the queue chunk holding pos (QueueChunk_impl.cuh:403-426).
-  // Returns kBehind when pos precedes `from`, kEmpty on timeout.
-  __device__ static uint32_t locate(HeapCore* h, uint32_t from, uint32_t pos) {
+  // `from` is a front_ptr / back_ptr value read a moment ago; the chunk may
+  // have been recycled since (front_ptr can pass many drained chunks at once),
+  // so every hop is checked: the chunk must carry the class's tag and the next
+  // range.  A failed check returns kStale (read the pointer again).  Returns
+  // kBehind when pos precedes `from`, kEmpty on timeout.
+  __device__ static uint32_t locate(HeapCore* h, ClassState* q, uint32_t from, uint32_t pos) {
+    const uint32_t tag = queue_tag(q);
+    const uint32_t want = pos / kQcSpots;
+    if (from >= h->max_chunks || ld_relaxed(&h->meta[from].size) != tag) return kStale;
     uint32_t cur = from, it = 0;
+    uint32_t vs = ld_relaxed(&h->meta[cur].vstart) / kQcSpots;
     for (uint32_t hops = 0; hops < (1u << 20); ++hops) {
-      uint32_t vs = ld_relaxed(&h->meta[cur].vstart) / kQcSpots;
-      uint32_t want = pos / kQcSpots;
-#ifdef OURO_SCAN_STATS
-      if (vs == want) atomicAdd(&h->scan[7].v, static_cast<unsigned long long>(hops));
-#endif
       if (vs == want) return cur;
       if (static_cast<int32_t>(want - vs) < 0) return kBehind;
-      uint32_t nx = next_of(h, cur, it);
+      const uint32_t nx = next_of(h, cur, it);
       if (nx == kEmpty) return kEmpty;
+      if (nx >= h->max_chunks || ld_relaxed(&h->meta[nx].size) != tag ||
+          ld_relaxed(&h->meta[nx].vstart) / kQcSpots != vs + 1u)
+        return kStale;
       cur = nx;
+      ++vs;
     }
-    note_timeout(h);
+    note_timeout(h, kWaitLocateHops);
     return kEmpty;
   }
 
   // locate() for a position the caller holds (its queue chunk cannot drain
-  // meanwhile), trying the index first.
-  __device__ static uint32_t locate_live(HeapCore* h, ClassState* q, uint32_t from, uint32_t pos) {
-    const uint32_t c = recall(h, q, pos);
-#ifdef OURO_SCAN_STATS
-    if (c == kEmpty) atomicAdd(&h->scan[3].v, 1ull);
-#endif
-    return c != kEmpty ? c : locate(h, from, pos);
+  // meanwhile), starting from *start (front_ptr or back_ptr).  The index is
+  // tried first and polled for a while: in a burst the chunk is usually being
+  // linked at that moment, and its linker enters it in the index as soon as it
+  // is attached, which beats walking the chain hop by hop behind it.
+  __device__ static uint32_t locate_live(HeapCore* h, ClassState* q, const uint32_t* start, uint32_t pos) {
+    for (uint32_t it = 0; it < kRecallPolls;) {
+      const uint32_t c = recall(h, q, pos);
+      if (c != kEmpty) return c;
+      backoff(it);
+    }
+    for (uint32_t attempt = 0; attempt < 64u; ++attempt) {
+      const uint32_t c = locate(h, q, ld_acquire(start), pos);
+      if (c != kStale) return c;
+      const uint32_t r = recall(h, q, pos);
+      if (r != kEmpty) return r;
+    }
+    note_timeout(h, kWaitLocateStale);
+    return kEmpty;
   }
 
   // The queue chunk after c, waiting for its link (and installing one when
@@ -425,7 +445,7 @@ struct VlStore {
     uint32_t* link = &h->meta[c].next;
     uint32_t nx;
     while ((nx = ld_acquire(link)) == kEmpty || nx == kInstalling) {
-      if (it >= kSpinLimit) { note_timeout(h); return kEmpty; }
+      if (it >= kSpinLimit) { note_timeout(h, kWaitLink); return kEmpty; }
       if (nx == kEmpty && it >= kInstallAfter && (it & 63u) == 0u) {
         uint32_t vs = ld_relaxed(&h->meta[c].vstart);
         install_queue_chunk(h, link, 0u, vs - vs % kQcSpots + kQcSpots,   // queue chunks always come from the base pool
@@ -620,16 +640,19 @@ struct VlStore {
 
   // A producer at the start of a queue chunk links the next one
   // (QueueChunk_impl.cuh:144-158).  A link needs its predecessor, so linking
-  // is a chain; when producers already hold positions several queue chunks
+  // is a chain.  When producers already hold positions several queue chunks
   // ahead (a burst), the group links up to one chunk per lane at once: one
-  // allocation for all, headers and links written in parallel, one CAS to
-  // attach the chain.  A lone producer is never more than one chunk ahead, so
-  // it links exactly one chunk, as the reference does.  c holds the range
-  // starting at pos.  Collective over g.
+  // allocation, headers and links written in parallel, one CAS to attach the
+  // piece, and index entries written right after, so that waiting producers
+  // find their chunk in the index instead of walking.  The producer at the
+  // start of the piece's last range continues the chain.  The piece is only
+  // ever attached to c, whose range the caller holds a position of: c cannot
+  // drain meanwhile.  (A chunk the caller does not hold may be drained,
+  // recycled and reused with an empty link, and a piece attached there would
+  // duplicate ranges of the live chain.)  A lone producer is never more than
+  // one chunk ahead, so it links exactly one chunk, as the reference does.
+  // c holds the range starting at pos.  Collective over g.
   __device__ static void preallocate(HeapCore* h, ClassState* q, const Group& g, uint32_t c, uint32_t pos) {
-#ifdef OURO_SCAN_STATS
-    const long long t0 = clock64();
-#endif
     uint32_t* link = &h->meta[c].next;
     uint32_t ahead = 0;
     if (g.is_leader() && ld_relaxed(link) == kEmpty) {
@@ -640,37 +663,37 @@ struct VlStore {
     }
     ahead = bcast(g, ahead);
     if (!ahead) return;
-    const uint32_t r = static_cast<uint32_t>(g.rank);
+    const uint32_t n = static_cast<uint32_t>(g.size), r = static_cast<uint32_t>(g.rank);
     uint32_t mine = kEmpty;
     const uint32_t got = alloc_chunks(h, g, ahead, q->inst, true, &mine);
     const bool have = r < got && mine != kEmpty;
     const uint32_t miss = __ballot_sync(g.mask, !have);
-    const uint32_t L = miss ? first_rank(g, miss) : static_cast<uint32_t>(g.size);
-    const uint32_t succ = __shfl_sync(g.mask, mine, lane_of_rank(g.mask, r + 1u < static_cast<uint32_t>(g.size)
-                                                                            ? static_cast<int>(r) + 1 : static_cast<int>(r)));
+    const uint32_t L = miss ? first_rank(g, miss) : n;
+    const uint32_t succ = __shfl_sync(g.mask, mine, lane_of_rank(g.mask, r + 1u < n ? static_cast<int>(r) + 1
+                                                                                   : static_cast<int>(r)));
+    const uint32_t vstart = pos + (r + 1u) * kQcSpots;
     if (r < L) {
-      init_queue_chunk(h, mine, pos + (r + 1u) * kQcSpots, queue_tag(q));
+      init_queue_chunk(h, mine, vstart, queue_tag(q));
       if (r + 1u < L) st_relaxed(&h->meta[mine].next, succ);
       __threadfence();
     } else if (have) {
-      reuse_put(h, &h->reuse[0], mine);
+      reuse_put(h, &h->reuse[0], mine);   // behind a hole: not part of the piece
     }
     __syncwarp(g.mask);
     if (L == 0u) return;
-    const uint32_t first = __shfl_sync(g.mask, mine, g.leader);
+    const uint32_t piece = __shfl_sync(g.mask, mine, g.leader);
     uint32_t ok = 0;
-    if (g.is_leader()) ok = atomicCAS(link, kEmpty, first) == kEmpty ? 1u : 0u;
+    if (g.is_leader()) ok = atomicCAS(link, kEmpty, piece) == kEmpty ? 1u : 0u;
     ok = bcast(g, ok);
     if (r < L) {
-      if (ok) remember(h, q, mine, pos + (r + 1u) * kQcSpots);
-      else reuse_put(h, &h->reuse[0], mine);
+      if (ok) {
+        remember(h, q, mine, vstart);
+      } else {   // someone else linked it: the piece goes back, untagged
+        st_relaxed(&h->meta[mine].size, 0u);
+        __threadfence();
+        reuse_put(h, &h->reuse[0], mine);
+      }
     }
-#ifdef OURO_SCAN_STATS
-    if (g.is_leader()) {
-      atomicAdd(&h->scan[10].v, 1ull);
-      atomicAdd(&h->scan[11].v, static_cast<unsigned long long>(clock64() - t0));
-    }
-#endif
   }
 
   __device__ static Group half_of(const Group& g, uint32_t pos, uint32_t first) {
@@ -684,7 +707,7 @@ struct VlStore {
                                        uint32_t chunk, uint32_t entries_per_chunk, Value&& value) {
     const uint32_t n = static_cast<uint32_t>(g.size);
     uint32_t c1 = kEmpty;
-    if (g.is_leader()) c1 = locate_live(h, q, ld_acquire(&q->back_ptr), b);
+    if (g.is_leader()) c1 = locate_live(h, q, &q->back_ptr, b);
     c1 = bcast(g, c1);
     if (c1 == kEmpty || c1 == kBehind) {
       if (g.is_leader()) set_status(h, kErrCorrupt);
@@ -721,7 +744,7 @@ struct VlStore {
   __device__ static void publish_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos, uint32_t v) {
     const uint32_t first = bcast(g, pos);
     uint32_t c1 = kEmpty;
-    if (g.is_leader()) c1 = locate_live(h, q, ld_acquire(&q->back_ptr), first);
+    if (g.is_leader()) c1 = locate_live(h, q, &q->back_ptr, first);
     c1 = bcast(g, c1);
     const Group sg = half_of(g, pos, first);
     if (c1 == kEmpty || c1 == kBehind) {
@@ -747,7 +770,7 @@ struct VlStore {
   __device__ static uint32_t consume_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos) {
     const uint32_t first = bcast(g, pos);
     uint32_t c1 = kEmpty;
-    if (g.is_leader()) c1 = locate_live(h, q, ld_acquire(&q->front_ptr), first);
+    if (g.is_leader()) c1 = locate_live(h, q, &q->front_ptr, first);
     c1 = bcast(g, c1);
     const Group sg = half_of(g, pos, first);
     if (c1 == kEmpty || c1 == kBehind) {
@@ -771,7 +794,7 @@ struct VlStore {
   // ---- chunk-queue side
   __device__ static bool enqueue_one(HeapCore* h, ClassState* q, uint32_t c, uint32_t* qpos) {
     uint32_t b = atomicAdd(&q->back.v, 1u);
-    uint32_t qc = locate_live(h, q, ld_acquire(&q->back_ptr), b);
+    uint32_t qc = locate_live(h, q, &q->back_ptr, b);
     if (qc == kEmpty || qc == kBehind) { set_status(h, kErrCorrupt); return false; }
     const Group self = make_group(1u << lane_id());
     if (b % kQcSpots == 0u) preallocate(h, q, self, qc, b);
@@ -791,7 +814,11 @@ struct VlStore {
       const uint32_t fp = ld_acquire(&q->front_ptr);
       const uint32_t fr = ld_relaxed(&h->meta[fp].vstart) / kQcSpots;
       const uint32_t cr = ld_relaxed(&h->meta[cur.chunk].vstart) / kQcSpots;
-      qc = locate(h, static_cast<int32_t>(cr - fr) < 0 ? fp : cur.chunk, pos);
+      qc = locate(h, q, static_cast<int32_t>(cr - fr) < 0 ? fp : cur.chunk, pos);
+      if (qc == kStale) {
+        cur.chunk = fp;
+        return kEmpty;
+      }
     }
     if (qc == kBehind) {
       cur.chunk = ld_acquire(&q->front_ptr);
@@ -802,7 +829,7 @@ struct VlStore {
     return ld_acquire(queue_slots(h, qc) + (pos % kQcSpots));
   }
   __device__ static void remove(HeapCore* h, ClassState* q, uint32_t pos) {
-    uint32_t qc = locate_live(h, q, ld_acquire(&q->front_ptr), pos);
+    uint32_t qc = locate_live(h, q, &q->front_ptr, pos);
     if (qc == kEmpty || qc == kBehind) return;
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
     __threadfence();
@@ -820,7 +847,8 @@ struct VlStore {
       from = f;
       if (static_cast<int32_t>(back - f) > 0) {
         const uint32_t first = ld_acquire(&q->front_ptr);
-        qc = locate(h, first, f);
+        qc = locate(h, q, first, f);
+        if (qc == kStale) qc = kEmpty;
         if (qc == kBehind) {
           // front lags the first live queue chunk: everything before it is gone
           const uint32_t vs = ld_relaxed(&h->meta[first].vstart);
