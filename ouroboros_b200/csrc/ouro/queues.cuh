@@ -249,74 +249,46 @@ __device__ bool chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32_t p
   return true;
 }
 
-// Cooperative claim of `got` free pages of chunk c for the group lanes in
-// `want` (in rank order).  The leader picks set bits in the order the
-// reference searches them for the leader's thread (ChunkAccess_impl.cuh:75-125:
-// first word (tid + 1) mod words, bits rotated by (tid + bid) mod 32), clears
-// them with one atomicAnd per word and the group distributes the won bits.
+// Cooperative claim of `got` free pages of chunk c for the unserved lanes of
+// s (in rank order).  The leader visits the mask words in the order the
+// reference searches them for the leader's thread (ChunkAccess_impl.cuh:
+// 75-125: first word (tid + 1) mod words, bits rotated by (tid + bid) mod 32),
+// one word at a time and stopping as soon as enough bits are won: it picks
+// the lowest set bits in rotated order, clears them with one atomicAnd, and
+// the group hands the won bits to its unserved lanes by rank.
 template <uint32_t W>
 __device__ void claim_pages(HeapCore* h, const Group& s, uint32_t c, uint32_t got, bool& served, uint32_t& page) {
   ChunkMeta* m = h->meta + c;
-  const uint32_t start = (threadIdx.x + 1u) % W;
-  const uint32_t offset = (threadIdx.x + blockIdx.x) % 32u;
-  const uint32_t start_b = bcast(s, start);
-  const uint32_t offset_b = bcast(s, offset);
+  const uint32_t start = bcast(s, (threadIdx.x + 1u) % W);
+  const uint32_t offset = bcast(s, (threadIdx.x + blockIdx.x) % 32u);
   uint32_t remaining = got;
   for (uint32_t attempt = 0; attempt < 64u && remaining; ++attempt) {
-    uint32_t words[W];
-    uint32_t won[W];
-    if (s.is_leader()) {
-      if constexpr (W == 16u) {
-#pragma unroll
-        for (uint32_t v = 0; v < 4u; ++v) {
-          uint4 x = ld_relaxed_v4(&m->mask[4u * v]);
-          words[4u * v] = x.x;
-          words[4u * v + 1u] = x.y;
-          words[4u * v + 2u] = x.z;
-          words[4u * v + 3u] = x.w;
-        }
-      } else {
-        words[0] = ld_relaxed(&m->mask[0]);
-      }
-      uint32_t left = remaining;
-#pragma unroll
-      for (uint32_t j = 0; j < W; ++j) {
-        const uint32_t w = (start + j) % W;
-        uint32_t word = 0u;
-#pragma unroll
-        for (uint32_t x = 0; x < W; ++x) word = x == w ? words[x] : word;
-        uint32_t rot = rotr32(word, offset);
-        uint32_t avail = __popc(rot);
-        uint32_t take = avail < left ? avail : left;
-        won[j] = 0u;
+    for (uint32_t j = 0; j < W && remaining; ++j) {
+      const uint32_t w = (start + j) % W;
+      uint32_t won = 0;
+      if (s.is_leader()) {
+        const uint32_t rot = rotr32(ld_relaxed(&m->mask[w]), offset);
+        const uint32_t avail = static_cast<uint32_t>(__popc(rot));
+        const uint32_t take = avail < remaining ? avail : remaining;
         if (take) {
-          uint32_t p = __fns(rot, 0u, static_cast<int>(take));
-          uint32_t picked_rot = rot & ((2u << p) - 1u);
-          uint32_t picked = rotl32(picked_rot, offset);
-          uint32_t old = atomicAnd(&m->mask[w], ~picked);
-          won[j] = picked & old;
-          left -= __popc(won[j]);
+          const uint32_t p = __fns(rot, 0u, static_cast<int>(take));
+          const uint32_t picked = rotl32(rot & ((2u << p) - 1u), offset);
+          won = picked & atomicAnd(&m->mask[w], ~picked);
         }
       }
-    }
-    // distribute the won bits to the unserved lanes in rank order
-    const uint32_t unserved = __ballot_sync(s.mask, !served);
-    const uint32_t u = __popc(unserved & ((1u << lane_id()) - 1u));
-    uint32_t base = 0;
-#pragma unroll
-    for (uint32_t j = 0; j < W; ++j) {
-      uint32_t wj = __shfl_sync(s.mask, s.is_leader() ? won[j] : 0u, s.leader);
-      uint32_t cnt = __popc(wj);
-      if (!served && u >= base && u < base + cnt) {
-        uint32_t rot = rotr32(wj, offset_b);
-        uint32_t p = __fns(rot, 0u, static_cast<int>(u - base + 1u));
-        uint32_t bit = (p + offset_b) % 32u;
-        page = ((start_b + j) % W) * 32u + bit;
+      won = bcast(s, won);
+      if (!won) continue;
+      // the u-th unserved lane takes the u-th won bit (in rotated order)
+      const uint32_t unserved = __ballot_sync(s.mask, !served);
+      const uint32_t u = static_cast<uint32_t>(__popc(unserved & ((1u << lane_id()) - 1u)));
+      const uint32_t cnt = static_cast<uint32_t>(__popc(won));
+      if (!served && u < cnt) {
+        const uint32_t p = __fns(rotr32(won, offset), 0u, static_cast<int>(u + 1u));
+        page = w * 32u + (p + offset) % 32u;
         served = true;
       }
-      base += cnt;
+      remaining -= cnt;
     }
-    remaining -= base;
   }
   if (remaining && s.is_leader()) set_status(h, kErrCorrupt);   // count promised pages the mask did not show
 }
@@ -400,12 +372,11 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
   Group s = make_group(smask);
   bool served = false;
   uint32_t page = 0, chunk = kEmpty;
-  uint32_t pos = 0, run_end = 0;
-  typename Store::Cursor cur{};
+  uint32_t pos = 0, run_end = 0, streak = 0;
+  typename Store::Cursor cur = Store::cursor(q);
   if (s.is_leader()) {
     pos = ld_relaxed(&q->front.v);
     run_end = pos + 1u;
-    cur = Store::cursor(q);
   }
   uint32_t need = static_cast<uint32_t>(s.size);
 #ifdef OURO_SCAN_STATS
@@ -445,7 +416,10 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
         if (!got) {
           OURO_STAT(st_miss);
           ++pos;
+          ++streak;
           if (static_cast<int32_t>(ld_relaxed(&q->back.v) - pos) <= 0) run_end = pos;   // next: a fresh run
+        } else {
+          streak = 0;
         }
       }
     }
@@ -477,8 +451,48 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
 #endif
       need = static_cast<uint32_t>(__popc(__ballot_sync(s.mask, !served)));
       if (need == 0u) break;
-    } else if (s.is_leader() && iter == 0u) {
-      run_end = pos;   // missed at the front: contended, switch to next-fit runs
+    } else {
+      if (s.is_leader() && iter == 0u) run_end = pos;   // missed at the front: contended, switch to next-fit runs
+      // Two misses in a row: the chunks with free pages have become sparse.
+      // Late in a burst they sit near the front (the front moves over removed
+      // entries), so the group sweeps from the front, one position per lane
+      // and round -- entry, page size, free count -- and the leader moves to
+      // the first chunk with free pages; after four empty rounds a fresh run.
+      if (bcast(s, streak >= 2u ? 1u : 0u)) {
+        uint32_t p0 = 0, back = 0;
+        if (s.is_leader()) {
+          p0 = ld_relaxed(&q->front.v);
+          back = ld_relaxed(&q->back.v);
+        }
+        p0 = bcast(s, p0);
+        back = bcast(s, back);
+        uint32_t m = 0, sweeps = 0;
+        for (; sweeps < 4u && !m && static_cast<int32_t>(back - p0) > 0; ++sweeps, p0 += static_cast<uint32_t>(s.size)) {
+          const uint32_t p = p0 + static_cast<uint32_t>(s.rank);
+          bool cand = false;
+          if (static_cast<int32_t>(back - p) > 0) {
+            const uint32_t v = Store::peek(h, q, p, cur);
+            if (v < h->max_chunks) {
+              const uint4 hd = ld_relaxed_v4(&h->meta[v].page_size);   // page_size, head, size, count
+              cand = hd.x == q->page_size && hd.y == 0u && static_cast<int32_t>(hd.w) > 0;
+            }
+          }
+          m = __ballot_sync(s.mask, cand);
+          if (m) break;
+        }
+        if (s.is_leader()) {
+          streak = 0;
+          if (m) {
+            pos = p0 + static_cast<uint32_t>(__popc(s.mask & ((1u << (__ffs(m) - 1)) - 1u)));
+            run_end = pos + 1u;
+          } else {
+            pos = run_end;   // nothing near the front: a fresh run next
+          }
+        }
+#ifdef OURO_SCAN_STATS
+        st_probe += static_cast<unsigned long long>(sweeps) * s.size;
+#endif
+      }
     }
   }
 #ifdef OURO_SCAN_STATS
