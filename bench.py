@@ -352,9 +352,11 @@ def roofline(res, n, steps) -> dict:
     distinct = ob.measure_atomics(0)
     peak = hot_lines * hot
     vidx = VARIANTS.index(v)
-    traffic = None
+    traffic, traffic_cell = None, None
     try:
-        traffic = json.load(open(TRAFFIC_FILE)).get(f"k_{kern}<{vidx}>")
+        t = json.load(open(TRAFFIC_FILE)).get(f"k_{kern}<{vidx}>")
+        if t:
+            traffic, traffic_cell = t["bytes"], t["cell"]
     except Exception:
         pass
     peaks = measured_peaks()
@@ -363,7 +365,7 @@ def roofline(res, n, steps) -> dict:
         "bound": "l2_atomic", "kernel": f"k_{kern}<{vidx}> ({v})", "share": round(ms_sum / total, 4),
         "achieved": round(achieved, 4), "peak": round(peak, 4), "unit": "G hot-line RMW/s",
         "frac": round(achieved / peak, 4), "traffic": traffic,
-        "traffic_unit": "bytes per launch (dram read + write, ncu)",
+        "traffic_unit": "bytes per launch (dram read + write, ncu)", "traffic_cell": traffic_cell,
         "peak_source": f"measured live by ouro_measure_atomics: one hot 32-bit address, one RMW per warp, "
                        f"x{hot_lines} independent hot lines",
         "avg_launch_ms": round(avg_ms, 5), "launches": launches,

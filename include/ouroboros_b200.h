@@ -173,6 +173,27 @@ typedef struct {
 } ouro_heap_report;
 int ouro_check_heap(ouro_heap* h, ouro_heap_report* out);
 
+/* Free resources of a heap (include/device/MemoryQueries.cuh:8-88
+ * printFreeResources, include/device/Statistics.h:30-57), as numbers instead
+ * of printf: per class its page size, the free pages its semaphore counts and
+ * the entries between its queue's front and back; overall the chunks in use
+ * (bump pointer minus pooled chunks), the chunks never handed out, the
+ * pooled ones, and free_bytes = sum of free pages x page size + (never handed
+ * out + pooled) x chunk size -- the figure an admission watermark compares
+ * against.  Reads the control block only; meaningful when no allocation is in
+ * flight.  Synchronous. */
+typedef struct {
+  uint32_t page_size[12];
+  int64_t free_pages[12];
+  uint64_t queue_entries[12];
+  uint64_t chunks_in_use;
+  uint64_t chunks_untouched;
+  uint64_t chunks_pooled;
+  uint64_t free_bytes;
+  uint64_t heap_chunks;     /* usable base chunks: max_chunks - 1 */
+} ouro_free_report;
+int ouro_free_resources(ouro_heap* h, ouro_free_report* out);
+
 /* Measured L2 atomic throughput of the current device, the roofline
  * reference of the allocator kernels (no counterpart in the reference):
  * mode 0 distinct addresses (atomics/s over all lanes), mode 1 one hot 32-bit

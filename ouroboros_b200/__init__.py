@@ -38,7 +38,7 @@ EXPORTS = (
     "ouro_create", "ouro_destroy", "ouro_device_handle", "ouro_get_info", "ouro_alloc", "ouro_free",
     "ouro_trace", "ouro_state", "ouro_get_status", "ouro_write_pattern", "ouro_verify_pattern",
     "ouro_check_allocations", "ouro_check_heap", "ouro_measure_atomics", "ouro_scan_stats",
-    "ouro_status_string", "ouro_check_allocations_noalloc",
+    "ouro_status_string", "ouro_check_allocations_noalloc", "ouro_free_resources",
 )
 
 
@@ -59,6 +59,13 @@ class _Status(ctypes.Structure):
 
 class _AllocReport(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("checked", "nulls", "out_of_heap", "misaligned", "overlaps")]
+
+
+class _FreeReport(ctypes.Structure):
+    _fields_ = [("page_size", ctypes.c_uint32 * 12), ("free_pages", ctypes.c_int64 * 12),
+                ("queue_entries", ctypes.c_uint64 * 12), ("chunks_in_use", ctypes.c_uint64),
+                ("chunks_untouched", ctypes.c_uint64), ("chunks_pooled", ctypes.c_uint64),
+                ("free_bytes", ctypes.c_uint64), ("heap_chunks", ctypes.c_uint64)]
 
 
 class _HeapReport(ctypes.Structure):
@@ -95,6 +102,7 @@ def lib():
         L.ouro_measure_atomics.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
         L.ouro_scan_stats.argtypes = [p, p, i]
         L.ouro_check_allocations_noalloc.argtypes = [p, p, u32, u32, p, p, p]
+        L.ouro_free_resources.argtypes = [p, ctypes.POINTER(_FreeReport)]
         L.ouro_status_string.argtypes = [i]
         L.ouro_status_string.restype = ctypes.c_char_p
         _lib = L
@@ -214,6 +222,19 @@ class Ouroboros:
         names = ("groups", "probes", "misses", "runs", "slow_cyc_sem", "slow_cyc_scan", "slow_cyc_dequeue",
                  "slow_cyc_claim", "slow_groups", "cyc_max", "slow_probes", "slow_misses")
         return {k: int(x) for k, x in zip(names, out)}
+
+    def free_resources(self) -> dict:
+        """printFreeResources (MemoryQueries.cuh:8-88) as numbers: per class
+        page size, free pages, queue entries; chunks in use / untouched /
+        pooled and the free bytes an admission watermark compares against."""
+        out = _FreeReport()
+        _check(lib().ouro_free_resources(self._handle(), ctypes.byref(out)), "ouro_free_resources")
+        return {
+            "page_size": list(out.page_size), "free_pages": list(out.free_pages),
+            "queue_entries": list(out.queue_entries), "chunks_in_use": int(out.chunks_in_use),
+            "chunks_untouched": int(out.chunks_untouched), "chunks_pooled": int(out.chunks_pooled),
+            "free_bytes": int(out.free_bytes), "heap_chunks": int(out.heap_chunks),
+        }
 
     def check_heap(self) -> dict:
         out = _HeapReport()

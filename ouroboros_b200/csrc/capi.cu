@@ -579,6 +579,33 @@ int ouro_check_heap(ouro_heap* h, ouro_heap_report* out) {
 }
 
 
+int ouro_free_resources(ouro_heap* h, ouro_free_report* out) {
+  if (!h || !out) return OURO_ERR_ARG;
+  if (cudaDeviceSynchronize() != cudaSuccess) return OURO_ERR_CUDA;
+  HeapCore core;
+  if (cudaMemcpy(&core, h->dev, sizeof(core), cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
+  std::memset(out, 0, sizeof(*out));
+  unsigned long long free_bytes = 0;
+  for (uint32_t c = 0; c < kNumClasses; ++c) {
+    const ClassState& q = core.cls[c];
+    out->page_size[c] = q.page_size;
+    out->free_pages[c] = SemWord::count(q.sem.v);
+    out->queue_entries[c] = static_cast<uint32_t>(q.back.v - q.front.v);
+    if (out->free_pages[c] > 0) free_bytes += static_cast<unsigned long long>(out->free_pages[c]) * q.page_size;
+  }
+  const unsigned long long usable = h->L.max_chunks - 1u;
+  const unsigned long long bumped = core.next_free_chunk.v < usable ? core.next_free_chunk.v : usable;
+  const long long pooled0 = core.reuse[0].count.v > 0 ? core.reuse[0].count.v : 0;
+  const long long pooled1 = core.reuse[1].count.v > 0 ? core.reuse[1].count.v : 0;
+  const unsigned long long pooled = static_cast<unsigned long long>(pooled0) + 4ull * static_cast<unsigned long long>(pooled1);
+  out->heap_chunks = usable;
+  out->chunks_untouched = usable - bumped;
+  out->chunks_pooled = pooled;
+  out->chunks_in_use = bumped > pooled ? bumped - pooled : 0;
+  out->free_bytes = free_bytes + (out->chunks_untouched + pooled) * kChunkBytes;
+  return OURO_OK;
+}
+
 // Diagnostic counters of the chunk-based allocation path (zero unless the
 // library was built with OURO_SCAN_STATS); no counterpart in the reference.
 int ouro_scan_stats(ouro_heap* h, uint64_t* out, int clear) {

@@ -41,6 +41,9 @@ constexpr uint32_t kInstallAfter = 256u;
 // of the window, the pre-allocated successor, one more for a front that
 // recycles late, and for linked queues the hold-back of drained chunks.
 __host__ __device__ constexpr uint32_t queue_margin(int kind) { return kind == 1 ? 4u : kind == 2 ? 4u + kOldHold : 0u; }
+// Removed entries a chunk queue may hold between front and back before a
+// free helps the front (frees alone never move it).
+constexpr uint32_t kFrontSlack = 4u * kQcSpots;
 // Slots of the linked queues' chunk index (recently linked queue chunks).
 constexpr uint32_t kSkipSlots = 1024u;
 

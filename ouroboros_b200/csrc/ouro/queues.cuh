@@ -300,11 +300,12 @@ __device__ uint32_t chunk_grow(HeapCore* h, ClassState* q, const Group& g, uint3
   const uint32_t factor = instance_factor(q->inst);
   uint32_t kk = k;
   if constexpr (Store::kKind != 0) {
-    // a chunk has at most one live entry; removed entries wait for the front:
-    // the budget counts two queue entries per chunk
+    // a chunk has at most one live entry; removed entries wait for the front
+    // and re-enqueued chunks take new positions: the budget counts three queue
+    // entries per chunk
     if (g.is_leader()) {
       const uint32_t old = atomicAdd(&q->class_chunks, k);
-      kk = commit_budget(h, k, factor, 2u * old, 2u);
+      kk = commit_budget(h, k, factor, 3u * old, 3u);
       if (kk < k) atomicSub(&q->class_chunks, k - kk);
     }
     kk = bcast(g, kk);
@@ -530,13 +531,19 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
   if (wg.is_leader()) atomicOr(&m->mask[page >> 5], bits);
   __syncwarp(cg.mask);
   __threadfence();
-  uint32_t flashed = 0;
+  uint32_t flashed = 0, help = 0;
   if (cg.is_leader()) {
     const int32_t n = cg.size;
     int32_t old = atomicAdd(&m->count, n);
     const int32_t size = static_cast<int32_t>(ld_relaxed(&m->size));
     if (old <= 0 && old + n > 0) {
       ensure_enqueued<Store>(h, q, c);
+      // frees only add entries at the back: when removed entries pile up
+      // ahead of the front (nothing has been allocating), move the front, so
+      // that the queue chunks behind it return to the pool
+      if (ld_relaxed(&q->back.v) - ld_relaxed(&q->front.v) >
+          static_cast<uint32_t>(ld_relaxed(&q->entries.v)) + kFrontSlack)
+        help = 1u;
     } else if (Standard && old + n == size && ld_relaxed(&q->entries.v) > kLowerFillC) {
       // ChunkQueue_impl.cuh:162-199: hand a fully free chunk back to the pool
       if (sem_try_reduce(q, static_cast<uint32_t>(size - n))) {
@@ -558,7 +565,8 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
     }
   }
   flashed = __shfl_sync(cg.mask, flashed, cg.leader);
-  if (flashed == 2u) help_front<Store>(h, q, cg);
+  help = __shfl_sync(cg.mask, help, cg.leader);
+  if (flashed == 2u || help) help_front<Store>(h, q, cg);
   __syncwarp(g.mask);
   __threadfence();
   uint32_t total = __reduce_add_sync(g.mask, flashed ? 0u : 1u);

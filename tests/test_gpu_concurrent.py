@@ -97,11 +97,11 @@ def test_out_of_memory_exact_count(v):
 def _budget_chunks(v, mc, ppc):
     """Data chunks a virtualized heap of mc chunks grants one class before its
     chunk budget is spent: budget = data chunks + the queue chunks for the
-    class's entries (pages, or two per chunk for chunk queues) + per class one
+    class's entries (pages, or three per chunk for chunk queues) + per class one
     initial queue chunk and a margin (4 for array queues, 14 for linked)."""
     margin = 4 if v.startswith("VA") else 14
     committed = 12 * (1 + margin)
-    per = ppc if v.endswith("P") else 2
+    per = ppc if v.endswith("P") else 3
     m = 0
     while committed + (m + 1) + -(-(m + 1) * per // 2048) <= mc - 1:
         m += 1
@@ -152,3 +152,28 @@ def test_burst_grows_past_one_queue_chunk(v, size):
             _idle(heap, v)
         st = heap.status()
         assert st["flags"] == 0 and st["timeouts"] == 0, st
+
+
+@pytest.mark.parametrize("v", ob.VARIANTS)
+def test_free_resources_accounting(v):
+    # free bytes = free pages x page size + chunks never handed out or pooled
+    # x 8 KiB: an allocation of n pages of one class takes exactly n x page
+    # size (plus, for the virtualized variants, the queue chunks it needed)
+    # and freeing them gives it all back
+    size, n = 256, 1 << 16
+    with ob.Ouroboros(v, GiB) as heap:
+        r0 = heap.free_resources()
+        assert r0["chunks_in_use"] == (0 if v in ("P", "C") else 12)   # one queue chunk per class
+        assert r0["free_bytes"] == (r0["heap_chunks"] - r0["chunks_in_use"]) * 8192
+        ptrs = _ptrs(n)
+        heap.alloc(ptrs, n, size)
+        torch.cuda.synchronize()
+        r1 = heap.free_resources()
+        assert r1["page_size"][4] == 256 and r1["free_pages"][4] >= 0
+        extra = r0["free_bytes"] - r1["free_bytes"] - n * size   # queue chunks the entries needed
+        assert extra % 8192 == 0 and 0 <= extra // 8192 <= (0 if v in ("P", "C") else 64), (r0, r1)
+        heap.free(ptrs, n)
+        torch.cuda.synchronize()
+        r2 = heap.free_resources()
+        assert r2["free_bytes"] == r1["free_bytes"] + n * size
+        assert r2["free_pages"][4] == r1["free_pages"][4] + n and r2["queue_entries"][4] > 0
