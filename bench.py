@@ -62,6 +62,9 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-path measurement")
+    ap.add_argument("--batched-n", type=int, default=1 << 22)
+    ap.add_argument("--batched-cycles", type=int, default=100)
     return ap.parse_args()
 
 
@@ -381,6 +384,79 @@ def roofline(res, n, steps) -> dict:
     }
 
 
+def batched_bench(n: int, cycles: int, stream) -> dict:
+    """The batched configuration: chunk-based virtualized-array heap of 8 GiB,
+    n requests with sizes log-uniform in [16, 8192] B rounded up to 16 B
+    (seeded).  Phase 1: all n allocated, then all freed -- by the batched
+    kernels and, for comparison, by the per-thread kernels on the same sizes
+    (warm heap, L2 flushed).  Phase 2: `cycles` churn cycles, each freeing a
+    hashed 50% and re-allocating new log-uniform sizes, captured as one CUDA
+    graph and replayed.  Launch shape from the autotuner."""
+    import ouroboros_b200 as ob
+    rng = np.random.default_rng(2024)
+    sz = np.exp(rng.uniform(np.log(16), np.log(8192), n))
+    sizes = torch.from_numpy(((np.ceil(sz / 16) * 16).astype(np.uint32)).view(np.int32)).cuda()
+    ptrs = torch.zeros(n, dtype=torch.int64, device="cuda")
+    flush = torch.zeros(64 << 20, dtype=torch.int32, device="cuda")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    out = {"workload": "VAC, 8 GiB heap, %d requests log-uniform 16..8192 B (rounded up to 16 B)" % n}
+    with ob.Ouroboros("VAC", 8 * GiB) as heap:
+        out["autotune"] = heap.autotune_batch(n=min(n, 1 << 20), lo=16, hi=8192)
+        res = {}
+        for name, alloc, free in (
+                ("batched", lambda: heap.alloc_batch(sizes, ptrs, n, stream=stream),
+                 lambda: heap.free_batch(ptrs, n, stream=stream)),
+                ("per_thread", lambda: heap.alloc(ptrs, n, 0, sizes, stream=stream),
+                 lambda: heap.free(ptrs, n, stream=stream))):
+            times = []
+            for rep in range(4):
+                with torch.cuda.stream(stream):
+                    flush.add_(1)
+                    ev[0].record(stream)
+                    alloc()
+                    ev[1].record(stream)
+                    flush.add_(1)
+                    ev[2].record(stream)
+                    free()
+                    ev[3].record(stream)
+                stream.synchronize()
+                if rep:   # the first repetition warms the heap
+                    times.append(ev[0].elapsed_time(ev[1]) + ev[2].elapsed_time(ev[3]))
+            res[name] = 2.0 * n / (np.mean(times) * 1e-3) / 1e6
+        out["phase1_mops"] = {k: round(v, 1) for k, v in res.items()}
+        out["phase1_speedup"] = round(res["batched"] / res["per_thread"], 3)
+        # phase 2: the live set, then `cycles` churn cycles replayed from one graph
+        with torch.cuda.stream(stream):
+            heap.alloc_batch(sizes, ptrs, n, stream=stream)
+        stream.synchronize()
+        sizes_live = sizes.clone()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            for c in range(cycles):
+                heap.realloc_batch(ptrs, sizes_live, n, seed=77, cycle=c + 1, fraction_permille=500,
+                                   dist=("loguniform", 16, 8192), stream=torch.cuda.current_stream())
+        for _ in range(2):   # replays keep churning the same live set
+            g.replay()
+        torch.cuda.synchronize()
+        st0 = heap.status()
+        ev[0].record(stream)
+        with torch.cuda.stream(stream):
+            g.replay()
+        ev[1].record(stream)
+        stream.synchronize()
+        ms = ev[0].elapsed_time(ev[1])
+        ops = 2.0 * 0.5 * n * cycles   # a picked request is one free and one malloc
+        st = heap.status()
+        out["phase2"] = {"cycles": cycles, "ms": round(ms, 3), "mops": round(ops / (ms * 1e-3) / 1e6, 1),
+                         "ms_per_cycle": round(ms / cycles, 4), "null_results": st["null_results"] - st0["null_results"],
+                         "flags": st["flags"]}
+        del g
+        with torch.cuda.stream(stream):
+            heap.free_batch(ptrs, n, stream=stream)
+        stream.synchronize()
+    return out
+
+
 def measured_peaks() -> dict:
     try:
         return json.load(open(MEASURED_PEAKS))
@@ -507,6 +583,11 @@ def main():
                           "what": "per cell: request sizes host->device (pinned), alloc launch, pointer array "
                                   "device->host, free launch, through the C ABI; after the timed repetitions"}
         out["roofline"] = roofline(res, n, args.steps)
+        if not args.no_batched:
+            try:
+                out["batched"] = batched_bench(args.batched_n, args.batched_cycles, stream)
+            except Exception as exc:   # reported, the headline stands
+                out["batched"] = {"error": str(exc)[:300]}
         if not args.no_cpu and rank == 0:
             out["cpu_baseline"] = cpu_baseline(cells, n, heap_bytes)
     if rank == 0:

@@ -173,6 +173,49 @@ typedef struct {
 } ouro_heap_report;
 int ouro_check_heap(ouro_heap* h, ouro_heap_report* out);
 
+/* Bulk pre-population of one size class (the reference's preFillQueue /
+ * enqueueInitialChunk, include/device/queues/page/PageQueue.cuh:42-49,
+ * PageQueue_impl.cuh:40-53, include/device/queues/chunk/ChunkQueue_impl.cuh:
+ * 69-77): adds ceil(pages / pages-per-chunk) fresh chunks to the class of
+ * `size` and publishes all their pages as free, warps adding 32 chunks at a
+ * time through the path an elected allocation takes.  A later burst of that
+ * class then starts without creating chunks.  *out_pages (may be NULL)
+ * receives the pages added: fewer when the heap runs out.  Sizes above
+ * 32 KiB (CUDA device heap) are refused.  Synchronizes `stream`. */
+int ouro_prefill(ouro_heap* h, uint64_t size, uint64_t pages, uint64_t* out_pages, void* stream);
+
+/* The batched path (no counterpart in the reference, whose only caller is its
+ * per-thread benchmark): persistent kernels serve n requests in tiles of
+ * 4 x block; each tile is binned by size class in shared memory and served in
+ * binned order, so the lanes of a warp ask for the same class and a warp's 32
+ * requests cost one semaphore and one ticket atomic.  block = 0 takes the
+ * shape ouro_autotune_batch picked (256 until then); else 128, 256, 512 or
+ * 1024.  Stream-ordered; the kernels keep no state between launches and can
+ * be captured in a CUDA graph.
+ *   ouro_alloc_batch:   d_out[i] = malloc(d_sizes[i])
+ *   ouro_free_batch:    free(d_ptrs[i]) (nullptr skipped)
+ *   ouro_realloc_batch: one churn cycle over a live set: request i is picked
+ *     with probability fraction_permille / 1000 (a hash of seed, cycle and i);
+ *     a picked request frees d_ptrs[i], draws a new size from *dist into
+ *     d_sizes[i] and allocates it into d_ptrs[i]. */
+typedef struct {
+  int kind;       /* 0: log-uniform in [lo, hi] rounded up to 16 B;
+                     1: Zipf(zipf_s) over the ten 16 B .. 8 KiB classes (rank 1 = 16 B) */
+  uint32_t lo, hi;
+  float zipf_s;
+} ouro_size_dist;
+int ouro_alloc_batch(ouro_heap* h, const uint32_t* d_sizes, void** d_out, uint32_t n, int block, void* stream);
+int ouro_free_batch(ouro_heap* h, void* const* d_ptrs, uint32_t n, int block, void* stream);
+int ouro_realloc_batch(ouro_heap* h, void** d_ptrs, uint32_t* d_sizes, uint32_t n, uint64_t seed, uint32_t cycle,
+                       uint32_t fraction_permille, const ouro_size_dist* dist, int block, void* stream);
+/* Autotuner of the batched path: times alloc + free batches of n log-uniform
+ * sizes in [lo, hi] on this heap for every block size (128 .. 1024) and
+ * resident blocks per SM (all that fit, 1, 2, 4), keeps the fastest as the
+ * heap's batched launch shape and reports it (Mops/s counts mallocs + frees).
+ * Uses the heap: call it on an idle heap.  Allocates scratch; synchronous. */
+int ouro_autotune_batch(ouro_heap* h, uint32_t n, uint32_t lo, uint32_t hi, int* out_block, int* out_per_sm,
+                        double* out_mops);
+
 /* Free resources of a heap (include/device/MemoryQueries.cuh:8-88
  * printFreeResources, include/device/Statistics.h:30-57), as numbers instead
  * of printf: per class its page size, the free pages its semaphore counts and

@@ -38,7 +38,8 @@ EXPORTS = (
     "ouro_create", "ouro_destroy", "ouro_device_handle", "ouro_get_info", "ouro_alloc", "ouro_free",
     "ouro_trace", "ouro_state", "ouro_get_status", "ouro_write_pattern", "ouro_verify_pattern",
     "ouro_check_allocations", "ouro_check_heap", "ouro_measure_atomics", "ouro_scan_stats",
-    "ouro_status_string", "ouro_check_allocations_noalloc", "ouro_free_resources",
+    "ouro_status_string", "ouro_check_allocations_noalloc", "ouro_free_resources", "ouro_prefill",
+    "ouro_alloc_batch", "ouro_free_batch", "ouro_realloc_batch", "ouro_autotune_batch",
 )
 
 
@@ -59,6 +60,10 @@ class _Status(ctypes.Structure):
 
 class _AllocReport(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("checked", "nulls", "out_of_heap", "misaligned", "overlaps")]
+
+
+class _SizeDist(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("lo", ctypes.c_uint32), ("hi", ctypes.c_uint32), ("zipf_s", ctypes.c_float)]
 
 
 class _FreeReport(ctypes.Structure):
@@ -103,6 +108,12 @@ def lib():
         L.ouro_scan_stats.argtypes = [p, p, i]
         L.ouro_check_allocations_noalloc.argtypes = [p, p, u32, u32, p, p, p]
         L.ouro_free_resources.argtypes = [p, ctypes.POINTER(_FreeReport)]
+        L.ouro_prefill.argtypes = [p, u64, u64, ctypes.POINTER(ctypes.c_uint64), p]
+        L.ouro_alloc_batch.argtypes = [p, p, p, u32, i, p]
+        L.ouro_free_batch.argtypes = [p, p, u32, i, p]
+        L.ouro_realloc_batch.argtypes = [p, p, p, u32, u64, u32, u32, ctypes.POINTER(_SizeDist), i, p]
+        L.ouro_autotune_batch.argtypes = [p, u32, u32, u32, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_double)]
         L.ouro_status_string.argtypes = [i]
         L.ouro_status_string.restype = ctypes.c_char_p
         _lib = L
@@ -222,6 +233,38 @@ class Ouroboros:
         names = ("groups", "probes", "misses", "runs", "slow_cyc_sem", "slow_cyc_scan", "slow_cyc_dequeue",
                  "slow_cyc_claim", "slow_groups", "cyc_max", "slow_probes", "slow_misses")
         return {k: int(x) for k, x in zip(names, out)}
+
+    # -- batched path ---------------------------------------------------------
+    def alloc_batch(self, sizes, out_ptrs, n: int, block: int = 0, stream=None):
+        """out_ptrs[i] = malloc(sizes[i]), binned by size class per tile."""
+        _check(lib().ouro_alloc_batch(self._handle(), _addr(sizes), _addr(out_ptrs), n, block, _stream(stream)),
+               "ouro_alloc_batch")
+
+    def free_batch(self, ptrs, n: int, block: int = 0, stream=None):
+        _check(lib().ouro_free_batch(self._handle(), _addr(ptrs), n, block, _stream(stream)), "ouro_free_batch")
+
+    def realloc_batch(self, ptrs, sizes, n: int, seed: int, cycle: int, fraction_permille: int,
+                      dist=("loguniform", 16, 8192), block: int = 0, stream=None):
+        """One churn cycle: a hashed fraction of the requests frees and reallocates
+        with a new size drawn from dist = ("loguniform", lo, hi) or ("zipf", s)."""
+        d = _SizeDist(0, dist[1], dist[2], 0.0) if dist[0] == "loguniform" else _SizeDist(1, 16, 8192, float(dist[1]))
+        _check(lib().ouro_realloc_batch(self._handle(), _addr(ptrs), _addr(sizes), n, seed & (2**64 - 1), cycle,
+                                        fraction_permille, ctypes.byref(d), block, _stream(stream)),
+               "ouro_realloc_batch")
+
+    def autotune_batch(self, n: int = 1 << 20, lo: int = 16, hi: int = 8192) -> dict:
+        b, s, m = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        _check(lib().ouro_autotune_batch(self._handle(), n, lo, hi, ctypes.byref(b), ctypes.byref(s), ctypes.byref(m)),
+               "ouro_autotune_batch")
+        return {"block": b.value, "blocks_per_sm": s.value, "mops": m.value}
+
+    def prefill(self, size: int, pages: int, stream=None) -> int:
+        """preFillQueue: add enough fresh chunks to the class of `size` for
+        `pages` free pages; returns the pages added."""
+        out = ctypes.c_uint64()
+        _check(lib().ouro_prefill(self._handle(), int(size), int(pages), ctypes.byref(out), _stream(stream)),
+               "ouro_prefill")
+        return int(out.value)
 
     def free_resources(self) -> dict:
         """printFreeResources (MemoryQueries.cuh:8-88) as numbers: per class

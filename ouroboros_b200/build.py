@@ -37,7 +37,7 @@ def sources() -> list[str]:
 
 
 def headers() -> list[str]:
-    return sorted(glob.glob(os.path.join(CSRC, "ouro", "*.cuh"))) + [
+    return sorted(glob.glob(os.path.join(CSRC, "ouro", "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))) + [
         os.path.join(os.path.dirname(HERE), "include", "ouroboros_b200.h")]
 
 

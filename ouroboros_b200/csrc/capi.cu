@@ -10,26 +10,30 @@
 #include <new>
 #include <vector>
 
-#include "../../include/ouroboros_b200.h"
-#include "ouro/ouroboros.cuh"
+#include "handle.h"
 
 using namespace ouro;
 
-struct ouro_heap {
-  int variant;
-  int device;
-  unsigned long long heap_bytes;
-  Layout L;
-  void* raw;
-  HeapCore* dev;
-  char* base;
-};
-
 namespace {
 
-inline int cuda_rc(cudaError_t e) { return e == cudaSuccess ? OURO_OK : OURO_ERR_CUDA; }
-
 // ------------------------------------------------------------------ kernels
+
+// Bulk pre-population: warps take up to 32 chunks of work at a time from a
+// counter and add them to class cls; d_done[0] counts the chunks added.
+template <int V>
+__global__ void k_prefill(Ouroboros<V>* mm, uint32_t cls, uint32_t chunks, uint32_t* d_next,
+                          unsigned long long* d_done) {
+  for (;;) {
+    uint32_t base = 0;
+    if (lane_id() == 0u) base = atomicAdd(d_next, 32u);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (base >= chunks) return;
+    const uint32_t k = chunks - base < 32u ? chunks - base : 32u;
+    const uint32_t got = mm->prefill(cls, k);
+    if (lane_id() == 0u) atomicAdd(d_done, static_cast<unsigned long long>(got));
+    if (got < k) return;   // out of chunks (or budget)
+  }
+}
 
 // Queue initialization of the virtualized variants (MemoryInitialization.cuh:91-119
 // with PageQueueVA_impl.cuh:11-28 / PageQueueVL_impl.cuh:11-30): one queue chunk
@@ -229,23 +233,6 @@ __global__ void k_peak_hot(uint32_t* a, unsigned long long* a64, int iters, int 
   }
   if (acc == 0x9E3779B9u) *sink = acc;
 }
-
-// ----------------------------------------------------------- dispatch helpers
-
-template <typename F>
-int dispatch(int variant, F&& f) {
-  switch (variant) {
-    case 0: return f(std::integral_constant<int, 0>{});
-    case 1: return f(std::integral_constant<int, 1>{});
-    case 2: return f(std::integral_constant<int, 2>{});
-    case 3: return f(std::integral_constant<int, 3>{});
-    case 4: return f(std::integral_constant<int, 4>{});
-    case 5: return f(std::integral_constant<int, 5>{});
-    default: return OURO_ERR_ARG;
-  }
-}
-
-inline unsigned grid_for(uint32_t n, int block) { return (n + static_cast<unsigned>(block) - 1u) / block; }
 
 bool g_heap_limit_set = false;
 
@@ -578,6 +565,39 @@ int ouro_check_heap(ouro_heap* h, ouro_heap_report* out) {
   return OURO_OK;
 }
 
+
+int ouro_prefill(ouro_heap* h, uint64_t size, uint64_t pages, uint64_t* out_pages, void* stream) {
+  if (!h) return OURO_ERR_ARG;
+  const int cls = size_class(size);
+  if (cls < 0) return OURO_ERR_ARG;   // served by the CUDA device heap, nothing to pre-populate
+  const uint32_t ppc = class_pages_per_chunk(static_cast<uint32_t>(cls));
+  const unsigned long long chunks = (pages + ppc - 1u) / ppc;
+  if (chunks >= h->L.max_chunks) return OURO_ERR_ARG;
+  if (out_pages) *out_pages = 0;
+  if (chunks == 0) return OURO_OK;
+  uint32_t* d = nullptr;
+  if (cudaMalloc(&d, 16) != cudaSuccess) return OURO_ERR_NOMEM;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(d, 0, 16, s);
+  if (e == cudaSuccess) {
+    dispatch(h->variant, [&](auto v) {
+      constexpr int V = decltype(v)::value;
+      const unsigned warps = static_cast<unsigned>((chunks + 31u) / 32u);
+      const unsigned blocks = warps < 148u * 8u ? (warps + 7u) / 8u : 148u;
+      k_prefill<V><<<blocks, 256, 0, s>>>(reinterpret_cast<Ouroboros<V>*>(h->dev), static_cast<uint32_t>(cls),
+                                          static_cast<uint32_t>(chunks), d,
+                                          reinterpret_cast<unsigned long long*>(d + 2));
+      return 0;
+    });
+    e = cudaGetLastError();
+  }
+  unsigned long long done = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&done, d + 2, sizeof(done), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(d);
+  if (out_pages) *out_pages = done * ppc;
+  return cuda_rc(e);
+}
 
 int ouro_free_resources(ouro_heap* h, ouro_free_report* out) {
   if (!h || !out) return OURO_ERR_ARG;

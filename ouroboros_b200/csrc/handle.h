@@ -1,0 +1,44 @@
+// handle.h -- the host-side heap handle and launch helpers shared by the
+// library's translation units (capi.cu, batch.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "../../include/ouroboros_b200.h"
+#include "ouro/ouroboros.cuh"
+
+struct ouro_heap {
+  int variant;
+  int device;
+  unsigned long long heap_bytes;
+  ouro::Layout L;
+  void* raw;
+  ouro::HeapCore* dev;
+  char* base;
+  int batch_block;    // batched path launch shape picked by ouro_autotune_batch (0: default)
+  int batch_per_sm;   // resident blocks per SM for it (0: as many as fit)
+};
+
+namespace ouro {
+
+inline int cuda_rc(cudaError_t e) { return e == cudaSuccess ? OURO_OK : OURO_ERR_CUDA; }
+
+inline unsigned grid_for(uint32_t n, int block) { return (n + static_cast<unsigned>(block) - 1u) / block; }
+
+// Run f with the instantiation index as a compile-time constant.
+template <typename F>
+int dispatch(int variant, F&& f) {
+  switch (variant) {
+    case 0: return f(std::integral_constant<int, 0>{});
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 5: return f(std::integral_constant<int, 5>{});
+    default: return OURO_ERR_ARG;
+  }
+}
+
+}  // namespace ouro

@@ -40,6 +40,20 @@ struct Ouroboros : HeapCore {
     else return chunk_alloc<Store>(this, q, g);
   }
 
+  // Bulk pre-population (the reference's preFillQueue / enqueueInitialChunk,
+  // PageQueue.cuh:42-49, PageQueue_impl.cuh:40-53, ChunkQueue_impl.cuh:69-77):
+  // the group adds k fresh chunks to class cls and publishes all their pages
+  // as free, through the same path an elected allocation takes (the semaphore
+  // is told to expect k chunks first).  Collective over the calling lanes of
+  // one warp, k <= their number.  Returns the chunks added.
+  __device__ __forceinline__ uint32_t prefill(uint32_t cls, uint32_t k) {
+    const Group g = make_group(__activemask());
+    ClassState* q = &this->cls[cls];
+    if (g.is_leader()) atomicAdd(&q->sem.v, static_cast<unsigned long long>(k) << SemWord::kExpShift);
+    if constexpr (kPageBased) return page_grow<Store>(this, q, g, k);
+    else return chunk_grow<Store>(this, q, g, k);
+  }
+
   __device__ __forceinline__ void free(void* ptr) {
     const uint32_t active = __activemask();
     char* p = static_cast<char*>(ptr);

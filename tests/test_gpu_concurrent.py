@@ -175,5 +175,29 @@ def test_free_resources_accounting(v):
         heap.free(ptrs, n)
         torch.cuda.synchronize()
         r2 = heap.free_resources()
-        assert r2["free_bytes"] == r1["free_bytes"] + n * size
+        back = r2["free_bytes"] - r1["free_bytes"]    # the pages, less queue chunks the frees needed
+        assert back % 8192 == 0 and 0 <= (n * size - back) // 8192 <= (0 if v in ("P", "C") else 64), (r1, r2)
         assert r2["free_pages"][4] == r1["free_pages"][4] + n and r2["queue_entries"][4] > 0
+
+
+@pytest.mark.parametrize("v", ob.VARIANTS)
+def test_prefill_serves_a_burst_without_new_chunks(v):
+    # preFillQueue at scale: the class's pages are published up front, so the
+    # burst that follows takes no new data chunk
+    size, n = 128, 1 << 18
+    with ob.Ouroboros(v, GiB) as heap:
+        added = heap.prefill(size, n)
+        assert added == n, added                       # 128 B: 64 pages per chunk, n a multiple
+        r = heap.free_resources()
+        assert r["free_pages"][3] == n and r["queue_entries"][3] == (n if v.endswith("P") else n // 64)
+        used = r["chunks_in_use"]
+        ptrs = _ptrs(n)
+        rep, nulls, bad = _round(heap, ptrs, n, size, seed=5)
+        assert nulls == 0 and bad == 0 and rep["overlaps"] == 0 and rep["misaligned"] == 0
+        r2 = heap.free_resources()
+        assert r2["chunks_in_use"] - used <= (0 if v in ("P", "C") else 32), (used, r2["chunks_in_use"])
+        assert r2["free_pages"][3] == n
+        _idle(heap, v)
+        assert heap.status()["flags"] == 0
+        with pytest.raises(ob.OuroError):
+            heap.prefill(1 << 20, 1)                  # above 32 KiB: the CUDA device heap's
