@@ -216,6 +216,34 @@ int ouro_realloc_batch(ouro_heap* h, void** d_ptrs, uint32_t* d_sizes, uint32_t 
 int ouro_autotune_batch(ouro_heap* h, uint32_t n, uint32_t lo, uint32_t hi, int* out_block, int* out_per_sm,
                         double* out_mops);
 
+/* The dynamic-graph workload of the serving loop (no counterpart in the
+ * reference; its consumer, ouroGraph, lives outside the reference tree).  A
+ * graph of nv vertices keeps vertex v's out-edges, degree[v] uint32 ids, in
+ * one allocation vptr[v] of 4 x degree[v] bytes.  Edge j of v is a hash of
+ * (seed, v, j), so a vertex's content depends only on its degree.
+ *   ouro_graph_init:  degrees from a power law P(d) ~ d^-alpha (1 <= d <= 1024),
+ *     blocks allocated through the batched path and filled; d_scratch holds nv
+ *     uint32; d_failed[0] += vertices left without a block.
+ *   ouro_graph_grow:  each named vertex moves to a block of twice its edges
+ *     (8 x d bytes, at most 8 KiB): malloc, copy, append, free.  Vertices may
+ *     repeat within and across concurrent calls: a growing vertex is locked
+ *     (bounded wait).  d_failed[0] += allocations that returned nullptr,
+ *     d_failed[1] += requests that gave up waiting for a vertex.
+ *   ouro_graph_check: d_out2[0] += a checksum of the named vertices' edges,
+ *     d_out2[1] += vertices whose edges differ from their recipe.
+ *   ouro_free_bytes_to: the heap's free bytes (free pages x page size + chunks
+ *     never handed out or pooled x 8 KiB) written by a kernel to *dst (device
+ *     or mapped pinned host memory) -- the admission watermark read without
+ *     synchronizing the device.
+ * All stream-ordered, no allocation. */
+int ouro_graph_init(ouro_heap* h, void** d_vptr, uint32_t* d_degree, uint32_t* d_scratch, uint32_t nv, uint64_t seed,
+                    float alpha, unsigned long long* d_failed, void* stream);
+int ouro_graph_grow(ouro_heap* h, void** d_vptr, uint32_t* d_degree, const uint32_t* d_vertices, uint32_t n, uint32_t nv,
+                    uint64_t seed, unsigned long long* d_failed, void* stream);
+int ouro_graph_check(void* const* d_vptr, const uint32_t* d_degree, const uint32_t* d_vertices, uint32_t n, uint32_t nv,
+                     uint64_t seed, unsigned long long* d_out2, void* stream);
+int ouro_free_bytes_to(ouro_heap* h, unsigned long long* dst, void* stream);
+
 /* Free resources of a heap (include/device/MemoryQueries.cuh:8-88
  * printFreeResources, include/device/Statistics.h:30-57), as numbers instead
  * of printf: per class its page size, the free pages its semaphore counts and

@@ -40,6 +40,7 @@ EXPORTS = (
     "ouro_check_allocations", "ouro_check_heap", "ouro_measure_atomics", "ouro_scan_stats",
     "ouro_status_string", "ouro_check_allocations_noalloc", "ouro_free_resources", "ouro_prefill",
     "ouro_alloc_batch", "ouro_free_batch", "ouro_realloc_batch", "ouro_autotune_batch",
+    "ouro_graph_init", "ouro_graph_grow", "ouro_graph_check", "ouro_free_bytes_to",
 )
 
 
@@ -112,6 +113,10 @@ def lib():
         L.ouro_alloc_batch.argtypes = [p, p, p, u32, i, p]
         L.ouro_free_batch.argtypes = [p, p, u32, i, p]
         L.ouro_realloc_batch.argtypes = [p, p, p, u32, u64, u32, u32, ctypes.POINTER(_SizeDist), i, p]
+        L.ouro_graph_init.argtypes = [p, p, p, p, u32, u64, ctypes.c_float, p, p]
+        L.ouro_graph_grow.argtypes = [p, p, p, p, u32, u32, u64, p, p]
+        L.ouro_graph_check.argtypes = [p, p, p, u32, u32, u64, p, p]
+        L.ouro_free_bytes_to.argtypes = [p, p, p]
         L.ouro_autotune_batch.argtypes = [p, u32, u32, u32, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_double)]
         L.ouro_status_string.argtypes = [i]

@@ -484,7 +484,14 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
         if (s.is_leader()) {
           streak = 0;
           if (m) {
-            pos = p0 + static_cast<uint32_t>(__popc(s.mask & ((1u << (__ffs(m) - 1)) - 1u)));
+            // groups that sweep at the same time see the same candidates: each
+            // takes one picked by a hash of its warp, so that they spread over
+            // the chunks instead of queueing for the first one (with one or two
+            // pages per chunk that convoy cost O(groups^2) probes)
+            const uint32_t k = (blockIdx.x * 0x9E3779B1u + (threadIdx.x >> 5) * 0x85EBCA77u + iter * 0xC2B2AE3Du) %
+                               static_cast<uint32_t>(__popc(m));
+            const uint32_t lane = __fns(m, 0u, static_cast<int>(k + 1u));
+            pos = p0 + static_cast<uint32_t>(__popc(s.mask & ((1u << lane) - 1u)));
             run_end = pos + 1u;
           } else {
             pos = run_end;   // nothing near the front: a fresh run next
