@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--batched-n", type=int, default=1 << 22)
     ap.add_argument("--batched-cycles", type=int, default=100)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop measurement")
+    ap.add_argument("--no-churn", action="store_true", help="skip the churn measurement")
+    ap.add_argument("--churn-rounds", type=int, default=1000)
     ap.add_argument("--serving-seconds", type=float, default=1.0)
     return ap.parse_args()
 
@@ -459,6 +461,63 @@ def batched_bench(n: int, cycles: int, stream) -> dict:
     return out
 
 
+def churn_bench(rounds: int, stream) -> dict:
+    """The churn configuration: chunk-based virtualized linked-list heap of
+    16 GiB; an initial live set of 2^21 allocations; `rounds` rounds, each
+    freeing a hashed 30% of the live set and allocating replacements with sizes
+    Zipf(1.2) over the ten 16 B..8 KiB classes (rank 1 = 16 B), through the
+    batched churn kernel.  Tracks failed allocations, chunk reuse and peak
+    occupancy; ownership / alignment / heap-bounds checks and a seeded payload
+    every 10 rounds and at the end, the accounting check at the end."""
+    import ouroboros_b200 as ob
+    n = 1 << 21
+    ptrs = torch.zeros(n, dtype=torch.int64, device="cuda")
+    sizes = torch.zeros(n, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+    dist = ("zipf", 1.2)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    out = {"workload": "VLC 16 GiB, live set 2^21, %d rounds of 30%% free + Zipf(1.2) re-allocation" % rounds}
+    with ob.Ouroboros("VLC", 16 * GiB) as heap:
+        with torch.cuda.stream(stream):
+            heap.realloc_batch(ptrs, sizes, n, seed=99, cycle=0, fraction_permille=1000, dist=dist, stream=stream)
+        stream.synchronize()
+        st0 = heap.status()
+        peak, checked, bad, overlaps, ms = 0, 0, 0, 0, 0.0
+        for r in range(1, rounds + 1):
+            ev[0].record(stream)
+            heap.realloc_batch(ptrs, sizes, n, seed=99, cycle=r, fraction_permille=300, dist=dist, stream=stream)
+            ev[1].record(stream)
+            stream.synchronize()
+            ms += ev[0].elapsed_time(ev[1])
+            if r % 10 == 0 or r == rounds:
+                peak = max(peak, heap.free_resources()["chunks_in_use"])
+                rep = heap.check_allocations(ptrs, n, sizes=sizes)
+                ob.write_pattern(ptrs, n, 0, r, sizes)
+                ob.verify_pattern(ptrs, n, cnt, 0, r, sizes)
+                torch.cuda.synchronize()
+                overlaps += rep["overlaps"] + rep["misaligned"] + rep["out_of_heap"]
+                checked += 1
+        st = heap.status()
+        nulls, badw = cnt.tolist()
+        with torch.cuda.stream(stream):
+            heap.free_batch(ptrs, n, stream=stream)
+        stream.synchronize()
+        hr = heap.check_heap()
+        idle = all(hr["sem_count"][c] == hr["owned_pages"][c] == hr["free_pages_meta"][c] and
+                   hr["sem_expected"][c] == 0 and hr["sem_reserved"][c] == 0 for c in range(12)) and hr["bad"] == 0
+        fr = heap.free_resources()
+    ops = 2.0 * 0.3 * n * rounds
+    out.update({
+        "rounds": rounds, "ms": round(ms, 2), "mops": round(ops / (ms * 1e-3) / 1e6, 1),
+        "failed_allocs": st["null_results"] - st0["null_results"], "flags": st["flags"],
+        "chunk_allocs_after_warmup": st["chunk_allocs"] - st0["chunk_allocs"],
+        "peak_chunks_in_use": peak, "heap_chunks": fr["heap_chunks"], "checks": checked,
+        "overlap_or_bounds_violations": overlaps, "payload_nulls": nulls, "payload_bad_words": badw,
+        "accounting_idle_after_free": bool(idle),
+    })
+    return out
+
+
 def serving_bench(seconds: float) -> dict:
     """The serving configuration: page-based virtualized-array heap of 32 GiB
     holding a 10M-vertex power-law graph (degree exponent 2.1, uint32 ids);
@@ -612,6 +671,11 @@ def main():
                           "what": "per cell: request sizes host->device (pinned), alloc launch, pointer array "
                                   "device->host, free launch, through the C ABI; after the timed repetitions"}
         out["roofline"] = roofline(res, n, args.steps)
+        if not args.no_churn:
+            try:
+                out["churn"] = churn_bench(args.churn_rounds, stream)
+            except Exception as exc:   # reported, the headline stands
+                out["churn"] = {"error": str(exc)[:300]}
         if not args.no_serving:
             try:
                 out["serving"] = serving_bench(args.serving_seconds)

@@ -116,38 +116,62 @@ __global__ void __launch_bounds__(BLOCK) k_graph_grow(Ouroboros<V>* mm, void** v
     for (int j = 0; j < kPer; ++j)
       if (bins[j] < kBins) order[off[bins[j]] + slot[j]] = static_cast<uint32_t>(t0 + static_cast<uint64_t>(j) * BLOCK + threadIdx.x);
     __syncthreads();
-    for (uint32_t k = threadIdx.x; k < off[kBins]; k += BLOCK) {
-      const uint32_t v = vertices[order[k]];
-      uint32_t d = 0, it = 0;
-      for (;;) {
-        d = atomicOr(&degree[v], kLock);
-        if (!(d & kLock)) break;
-        if (it >= kSpinLimit) break;
-        backoff(it);
+    // Warps walk the binned order together: a lane takes a request, locks its
+    // vertex (one attempt per round, so two lanes of a warp naming the same
+    // vertex cannot wait on each other) and allocates the new block; then the
+    // whole warp copies and appends the edges of every request won this round,
+    // 32 edges at a time, so a warp does not wait on its largest vertex.
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t kb = threadIdx.x - lane; kb < off[kBins]; kb += BLOCK) {
+      const uint32_t k = kb + lane;
+      uint32_t v = 0;
+      bool pending = k < off[kBins];
+      if (pending) v = vertices[order[k]];
+      for (uint32_t round = 0, it = 0; __any_sync(0xFFFFFFFFu, pending); ++round) {
+        bool won = false;
+        uint32_t d = 0, nd = 0;
+        uint32_t* p = nullptr;
+        const uint32_t* old = nullptr;
+        if (pending) {
+          d = atomicOr(&degree[v], kLock);
+          if (!(d & kLock)) {
+            __threadfence();
+            pending = false;
+            nd = 2u * d < kMaxEdges ? 2u * d : kMaxEdges;
+            if (d >= kMaxEdges) {
+              st_release(&degree[v], d);   // full: nothing to grow
+            } else if ((p = static_cast<uint32_t*>(mm->malloc(4u * nd))) == nullptr) {
+              atomicAdd(&failed[0], 1ull);
+              st_release(&degree[v], d);
+            } else {
+              old = static_cast<const uint32_t*>(vptr[v]);
+              won = true;
+            }
+          } else if (round >= kSpinLimit) {   // gave up waiting for the vertex
+            atomicAdd(&failed[1], 1ull);
+            pending = false;
+          }
+        }
+        for (uint32_t m = __ballot_sync(0xFFFFFFFFu, won); m; m &= m - 1u) {
+          const int src = __ffs(m) - 1;
+          uint32_t* pl = reinterpret_cast<uint32_t*>(__shfl_sync(0xFFFFFFFFu, reinterpret_cast<unsigned long long>(p), src));
+          const uint32_t* ol =
+              reinterpret_cast<const uint32_t*>(__shfl_sync(0xFFFFFFFFu, reinterpret_cast<unsigned long long>(old), src));
+          const uint32_t dl = __shfl_sync(0xFFFFFFFFu, d, src), ndl = __shfl_sync(0xFFFFFFFFu, nd, src);
+          const uint32_t vl = __shfl_sync(0xFFFFFFFFu, v, src);
+          for (uint32_t j = lane; j < dl; j += 32u) pl[j] = ol[j];
+          for (uint32_t j = dl + lane; j < ndl; j += 32u) pl[j] = edge_of(seed, vl, j, nv);
+        }
+        __threadfence();   // every lane's edges are visible before a winner publishes its block
+        __syncwarp();
+        if (won) {
+          mm->free(const_cast<uint32_t*>(old));
+          vptr[v] = p;
+          __threadfence();
+          st_release(&degree[v], nd);   // releases the vertex
+        }
+        if (__any_sync(0xFFFFFFFFu, pending)) backoff(it);
       }
-      if (d & kLock) {   // gave up waiting
-        atomicAdd(&failed[1], 1ull);
-        continue;
-      }
-      __threadfence();
-      if (d >= kMaxEdges) {   // full: nothing to grow
-        st_release(&degree[v], d);
-        continue;
-      }
-      const uint32_t nd = 2u * d < kMaxEdges ? 2u * d : kMaxEdges;
-      uint32_t* p = static_cast<uint32_t*>(mm->malloc(4u * nd));
-      if (!p) {
-        atomicAdd(&failed[0], 1ull);
-        st_release(&degree[v], d);
-        continue;
-      }
-      const uint32_t* old = static_cast<const uint32_t*>(vptr[v]);
-      for (uint32_t j = 0; j < d; ++j) p[j] = old[j];
-      for (uint32_t j = d; j < nd; ++j) p[j] = edge_of(seed, v, j, nv);
-      mm->free(const_cast<uint32_t*>(old));
-      vptr[v] = p;
-      __threadfence();
-      st_release(&degree[v], nd);   // releases the vertex
     }
     __syncthreads();
   }
