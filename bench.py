@@ -427,6 +427,9 @@ def batched_bench(n: int, cycles: int, stream) -> dict:
                 if rep:   # the first repetition warms the heap
                     times.append(ev[0].elapsed_time(ev[1]) + ev[2].elapsed_time(ev[3]))
             res[name] = 2.0 * n / (np.mean(times) * 1e-3) / 1e6
+        st1 = heap.status(clear=True)
+        out["phase1_status"] = {"flags": st1["flags"], "timeout_sites": st1["timeout_sites"],
+                                "null_results": st1["null_results"]}
         out["phase1_mops"] = {k: round(v, 1) for k, v in res.items()}
         out["phase1_speedup"] = round(res["batched"] / res["per_thread"], 3)
         # phase 2: the live set, then `cycles` churn cycles replayed from one graph
@@ -453,7 +456,7 @@ def batched_bench(n: int, cycles: int, stream) -> dict:
         st = heap.status()
         out["phase2"] = {"cycles": cycles, "ms": round(ms, 3), "mops": round(ops / (ms * 1e-3) / 1e6, 1),
                          "ms_per_cycle": round(ms / cycles, 4), "null_results": st["null_results"] - st0["null_results"],
-                         "flags": st["flags"]}
+                         "flags": st["flags"], "timeout_sites": st["timeout_sites"], "timeouts": st["timeouts"]}
         del g
         with torch.cuda.stream(stream):
             heap.free_batch(ptrs, n, stream=stream)
@@ -671,17 +674,18 @@ def main():
                           "what": "per cell: request sizes host->device (pinned), alloc launch, pointer array "
                                   "device->host, free launch, through the C ABI; after the timed repetitions"}
         out["roofline"] = roofline(res, n, args.steps)
-        if not args.no_churn:
+        extras = rank == 0   # the configurations beyond the headline: one replica measures them
+        if extras and not args.no_churn:
             try:
                 out["churn"] = churn_bench(args.churn_rounds, stream)
             except Exception as exc:   # reported, the headline stands
                 out["churn"] = {"error": str(exc)[:300]}
-        if not args.no_serving:
+        if extras and not args.no_serving:
             try:
                 out["serving"] = serving_bench(args.serving_seconds)
             except Exception as exc:   # reported, the headline stands
                 out["serving"] = {"error": str(exc)[:300]}
-        if not args.no_batched:
+        if extras and not args.no_batched:
             try:
                 out["batched"] = batched_bench(args.batched_n, args.batched_cycles, stream)
             except Exception as exc:   # reported, the headline stands
