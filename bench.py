@@ -555,18 +555,35 @@ def measured_peaks() -> dict:
         return {}
 
 
+def replica_value(total_ms: float, e2e_ms: float, ops_per_rank: float, world: int, dist=None, device="cuda"):
+    """Replicas: every rank runs the whole workload on its own GPU.  The job's
+    time is the slowest rank's (a MAX all-reduce of the summed kernel times)
+    and its value all ranks' operations over that time.  Returns (Mops/s,
+    max total ms, max end-to-end ms)."""
+    if dist is not None and world > 1:
+        t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_ms = float(t[0].item()), float(t[1].item())
+    return ops_per_rank * world / (total_ms * 1e-3) / 1e6, total_ms, e2e_ms
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference" and world > 1:
+        # the reference arm is measured by rank 0 alone; the other ranks have no work
+        if rank != 0:
+            return 0
+        world = 1
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
 
     variants = [v for v in args.variants.split(",") if v]
     sizes = [int(s) for s in args.sizes.split(",") if s]
@@ -620,12 +637,7 @@ def main():
         if e is not None:
             e2e_ms += e
     nulls, bad = counters.tolist()
-    if dist:
-        t = torch.tensor([total_ms, e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_ms = float(t[0].item()), float(t[1].item())
-    ops_total = 2.0 * n * len(cells) * args.steps * world
-    value = ops_total / (total_ms * 1e-3) / 1e6
+    value, total_ms, e2e_ms = replica_value(total_ms, e2e_ms, 2.0 * n * len(cells) * args.steps, world, dist)
 
     # --- extra cells (ours only): 4096 / 8192 B exceed the heap for 2^20 requests
     extra = {}

@@ -1,5 +1,5 @@
 /*
- * host_replay.c -- BASELINE INFRASTRUCTURE ONLY.
+ * host_replay.c -- host-allocator baseline, test and benchmark infrastructure only.
  *
  * The request pattern of one benchmark cell (n requests of one size, or a
  * size per request) replayed through the host's glibc malloc/free with T

@@ -47,7 +47,7 @@ def test_trace_bit_exact(v, name):
     assert sbad.size == 0, f"state words differ: {sbad.tolist()}"
 
 
-def test_layout_survey_points():
+def test_layout_reference_points():
     # maxChunks quoted for the reference at 1/4/8/16/32 GiB (host probe of the
     # reference types): P/C, VA, VL
     want = {"P": [80596, 467763, 983985, 2016429, 4081317],
