@@ -205,6 +205,33 @@ __device__ void chunk_enqueue(HeapCore* h, ClassState* q, uint32_t c) {
   }
 }
 
+// chunk_enqueue for the lanes of g, one chunk each, whose queue_pos the
+// lanes have already moved from kEmpty to kPending: one reservation of g.size
+// entries and back positions for the whole group instead of one per chunk.
+template <class Store>
+__device__ void chunk_enqueue_group(HeapCore* h, ClassState* q, const Group& g, uint32_t c) {
+  const uint32_t n = static_cast<uint32_t>(g.size);
+  uint32_t b = 0, full = 0;
+  if (g.is_leader()) {
+    const int32_t fill = atomicAdd(&q->entries.v, static_cast<int32_t>(n));
+    if (static_cast<uint32_t>(fill) + n > chunk_queue_cap(Store::kKind)) {
+      atomicSub(&q->entries.v, static_cast<int32_t>(n));
+      set_status(h, kErrQueueFull);
+      full = 1u;
+    } else {
+      b = atomicAdd(&q->back.v, n);
+    }
+  }
+  if (bcast(g, full)) {
+    st_relaxed(&h->meta[c].queue_pos, kEmpty);
+    return;
+  }
+  const uint32_t pos = bcast(g, b) + static_cast<uint32_t>(g.rank);
+  st_relaxed(&h->meta[c].queue_pos, pos);
+  __threadfence();   // queue_pos before the entry: a consumer that finds the entry can remove it
+  Store::template publish_lane<false>(h, q, g, pos, c);
+}
+
 // A chunk whose count rose above zero must be findable: enqueue it unless it
 // still has (or is getting) an entry.  The reference does this on the first
 // free of a full chunk (ChunkQueue_impl.cuh:157-161).
@@ -226,7 +253,6 @@ __device__ void help_front(HeapCore* h, ClassState* q, const Group& g) {
   if (g.is_leader()) {
     __threadfence();
     atomicExch(&q->advancing.v, 0u);
-
   }
 }
 
@@ -325,11 +351,9 @@ __device__ uint32_t chunk_grow(HeapCore* h, ClassState* q, const Group& g, uint3
   }
   __syncwarp(g.mask);
   __threadfence();
-  // one entry per chunk, in rank order (k <= group size)
-  for (uint32_t r = 0; r < got; ++r) {
-    uint32_t cr = __shfl_sync(g.mask, c, lane_of_rank(g.mask, static_cast<int>(r)));
-    if (g.is_leader() && cr != kEmpty) chunk_enqueue<Store>(h, q, cr);
-  }
+  // one entry per chunk, in rank order (k <= group size), reserved together
+  const uint32_t em = __ballot_sync(g.mask, mine);
+  if (mine) chunk_enqueue_group<Store>(h, q, make_group(em), c);
   __syncwarp(g.mask);
   __threadfence();
   if (g.is_leader()) sem_fulfil(q, got * q->ppc, k);
@@ -345,6 +369,74 @@ __device__ uint32_t claim_run(HeapCore* h, ClassState* q, uint32_t run) {
   const uint32_t w = ld_relaxed(&q->back.v) - f;
   if (static_cast<int32_t>(w) <= 0) return f;
   return f + (c - f) % w;
+}
+
+// Exclusive prefix sum of v over the ranks of group g.
+__device__ __forceinline__ uint32_t group_exclusive_sum(const Group& g, uint32_t v) {
+  uint32_t incl = v;
+  const int r = g.rank;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t other = __shfl_sync(g.mask, incl, lane_of_rank(g.mask, r >= d ? r - d : r));
+    if (d < g.size && r >= d) incl += other;
+  }
+  return incl - v;
+}
+
+// A group that needs several chunks' worth of pages (more lanes than a chunk
+// has pages) takes one run of that many positions from the scan cursor and
+// works it in parallel: lane r examines position r of the run (entry, page
+// size, free count), reserves on its chunk what the group still needs after
+// the lanes below it, the pages are claimed chunk by chunk and the takers of a
+// chunk's last pages remove its entry.  Whatever the run could not serve is
+// left to the probe loop.
+template <class Store>
+__device__ void chunk_alloc_run(HeapCore* h, ClassState* q, const Group& s, typename Store::Cursor& cur,
+                                uint32_t run, bool& served, uint32_t& page, uint32_t& chunk) {
+  const uint32_t r = static_cast<uint32_t>(s.rank);
+  const uint32_t need = static_cast<uint32_t>(s.size);
+  uint32_t base = 0, back = 0;
+  if (s.is_leader()) {
+    base = claim_run<Store>(h, q, run);
+    back = ld_relaxed(&q->back.v);
+  }
+  base = bcast(s, base);
+  back = bcast(s, back);
+  const uint32_t pos = base + r;
+  uint32_t v = kEmpty, cnt = 0;
+  if (r < run && static_cast<int32_t>(back - pos) > 0) {
+    v = Store::peek(h, q, pos, cur);
+    if (v < h->max_chunks) {
+      const uint4 hd = ld_relaxed_v4(&h->meta[v].page_size);   // page_size, head, size, count
+      if (hd.x == q->page_size && hd.y == 0u && static_cast<int32_t>(hd.w) > 0) cnt = hd.w;
+    }
+  }
+  const uint32_t before = group_exclusive_sum(s, cnt);
+  uint32_t want = need > before ? need - before : 0u;
+  if (want > cnt) want = cnt;
+  uint32_t got = 0;
+  bool last = false;
+  if (want) {
+    const int32_t old = atomicSub(&h->meta[v].count, static_cast<int32_t>(want));
+    got = old <= 0 ? 0u : (static_cast<uint32_t>(old) < want ? static_cast<uint32_t>(old) : want);
+    if (got < want) {
+      const int32_t give = static_cast<int32_t>(want - got);
+      const int32_t prev = atomicAdd(&h->meta[v].count, give);
+      if (prev <= 0 && prev + give > 0) ensure_enqueued<Store>(h, q, v);
+    }
+    last = got > 0u && old <= static_cast<int32_t>(want);
+  }
+  for (uint32_t m = __ballot_sync(s.mask, got > 0u); m; m &= m - 1u) {
+    const int src = __ffs(m) - 1;
+    const uint32_t c = __shfl_sync(s.mask, v, src);
+    const uint32_t k = __shfl_sync(s.mask, got, src);
+    const bool was = served;
+    if (q->inst == 0u) claim_pages<16u>(h, s, c, k, served, page);
+    else claim_pages<1u>(h, s, c, k, served, page);
+    if (served && !was) chunk = c;
+  }
+  const bool removed = last && chunk_dequeue<Store>(h, q, v, pos);
+  if (__ballot_sync(s.mask, removed)) help_front<Store>(h, q, s);
 }
 
 // ChunkQueue_impl.cuh:82-148 allocPage, for a group.  The first probe is the
@@ -375,11 +467,34 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
   uint32_t page = 0, chunk = kEmpty;
   uint32_t pos = 0, run_end = 0, streak = 0;
   typename Store::Cursor cur = Store::cursor(q);
+  uint32_t need = static_cast<uint32_t>(s.size);
+  {
+    const uint32_t run = (need + q->ppc - 1u) / q->ppc;
+    if (run > 1u) {
+      chunk_alloc_run<Store>(h, q, s, cur, run, served, page, chunk);
+      // the whole group stays in the probe loop, served lanes included: its
+      // sweeps cover one position per lane of the group, not of the rest
+      need = static_cast<uint32_t>(__popc(__ballot_sync(s.mask, !served)));
+      if (need == 0u) {
+#ifdef OURO_SCAN_STATS
+        if (s.is_leader()) {   // served by the run: slow ones are counted with the slow probe-loop groups
+          const unsigned long long total = static_cast<unsigned long long>(clock64() - t_begin);
+          if (total > (1ull << 19)) {
+            atomicAdd(&h->scan[4].v, static_cast<unsigned long long>(t_sem));
+            atomicAdd(&h->scan[5].v, total - static_cast<unsigned long long>(t_sem));
+            atomicAdd(&h->scan[8].v, 1ull);
+          }
+          atomicMax(&h->scan[9].v, total);
+        }
+#endif
+        return page_address(h, chunk, page, q->page_shift);
+      }
+    }
+  }
   if (s.is_leader()) {
     pos = ld_relaxed(&q->front.v);
     run_end = pos + 1u;
   }
-  uint32_t need = static_cast<uint32_t>(s.size);
 #ifdef OURO_SCAN_STATS
   unsigned long long st_probe = 0, st_miss = 0, st_run = 0;
 #define OURO_STAT(x) ++(x)
@@ -481,6 +596,9 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
           m = __ballot_sync(s.mask, cand);
           if (m) break;
         }
+        // nothing with free pages near the front: removed entries may hide
+        // them there, so the group moves the front before its next run
+        if (!m) help_front<Store>(h, q, s);
         if (s.is_leader()) {
           streak = 0;
           if (m) {
@@ -538,13 +656,14 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
   if (wg.is_leader()) atomicOr(&m->mask[page >> 5], bits);
   __syncwarp(cg.mask);
   __threadfence();
-  uint32_t flashed = 0, help = 0;
+  uint32_t flashed = 0, help = 0, enq = 0;
   if (cg.is_leader()) {
     const int32_t n = cg.size;
     int32_t old = atomicAdd(&m->count, n);
     const int32_t size = static_cast<int32_t>(ld_relaxed(&m->size));
     if (old <= 0 && old + n > 0) {
-      ensure_enqueued<Store>(h, q, c);
+      // the chunk needs an entry unless it still has (or is getting) one
+      enq = atomicCAS(&m->queue_pos, kEmpty, kPending) == kEmpty ? 1u : 0u;
       // frees only add entries at the back: when removed entries pile up
       // ahead of the front (nothing has been allocating), move the front, so
       // that the queue chunks behind it return to the pool
@@ -571,6 +690,9 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
       }
     }
   }
+  // the chunks of the warp that need an entry are enqueued together
+  const uint32_t em = __ballot_sync(g.mask, enq != 0u);
+  if (enq) chunk_enqueue_group<Store>(h, q, make_group(em), c);
   flashed = __shfl_sync(cg.mask, flashed, cg.leader);
   help = __shfl_sync(cg.mask, help, cg.leader);
   if (flashed == 2u || help) help_front<Store>(h, q, cg);

@@ -108,6 +108,7 @@ struct FlatStore {
     }
   }
 
+  template <bool PageQueue = true>
   __device__ static void publish_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos, uint32_t v) {
     uint32_t* s = slot(q, pos);
     if (wait_slot_empty(h, s)) st_relaxed(s, v);
@@ -251,6 +252,9 @@ struct VaStore {
     }
   }
 
+  // PageQueue false: a chunk queue, whose queue chunks return to the pool
+  // from the front (advance_front), not when their entries are consumed.
+  template <bool PageQueue = true>
   __device__ static void publish_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos, uint32_t v) {
     const Group sg = half_of(g, pos, bcast(g, pos));
     if (pos % kQcSpots == 0u) preallocate(h, q, pos);
@@ -263,7 +267,7 @@ struct VaStore {
     }
     __syncwarp(sg.mask);
     __threadfence();
-    if (sg.is_leader() && qc != kEmpty) count_enqueued(h, q, qc, pos, static_cast<uint32_t>(sg.size), true);
+    if (sg.is_leader() && qc != kEmpty) count_enqueued(h, q, qc, pos, static_cast<uint32_t>(sg.size), PageQueue);
   }
 
   __device__ static uint32_t consume_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos) {
@@ -741,6 +745,7 @@ struct VlStore {
     }
   }
 
+  template <bool PageQueue = true>
   __device__ static void publish_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos, uint32_t v) {
     const uint32_t first = bcast(g, pos);
     uint32_t c1 = kEmpty;
