@@ -467,20 +467,46 @@ struct VlStore {
   // QueueChunk_impl.cuh:440-463 setBackPointer.  back_ptr, where locate()
   // starts for producers, moves over full queue chunks whose successor is
   // linked.  Every walk starts from the current back_ptr and publishes with
-  // one CAS, so a chunk that fills while another lane walks is passed by one
-  // of the two.
-  __device__ static void set_back(HeapCore* h, ClassState* q) {
-    uint32_t bp = ld_acquire(&q->back_ptr);
+  // one CAS, so a chunk that fills while another group walks is passed by one
+  // of the two.  Chunks fill out of order in a burst, so the filler of the
+  // oldest one may have hundreds to pass: the group looks at one queue chunk
+  // per lane and round, lane i at the range i after the walk's position,
+  // found through the index and checked against its predecessor's link (a
+  // chunk the index does not hold ends the round; the next round starts from
+  // the real link, so a round passes at least one chunk).  Collective over g.
+  __device__ static void set_back(HeapCore* h, ClassState* q, const Group& g) {
+    const uint32_t n = static_cast<uint32_t>(g.size), r = static_cast<uint32_t>(g.rank);
+    const uint32_t tag = queue_tag(q);
+    uint32_t bp = 0;
+    if (g.is_leader()) bp = ld_acquire(&q->back_ptr);
+    bp = bcast(g, bp);
     for (uint32_t round = 0; round < 64u; ++round) {
       uint32_t cur = bp;
-      for (uint32_t i = 0; i < (1u << 16); ++i) {
-        if ((ld_acquire(&h->meta[cur].qcount) & 0xFFFFu) != kQcSpots) break;
-        const uint32_t nx = ld_acquire(&h->meta[cur].next);
-        if (nx >= kInstalling) break;
-        cur = nx;
+      for (uint32_t step = 0; step < (1u << 16); ++step) {
+        uint32_t r0 = 0;
+        if (g.is_leader()) r0 = ld_relaxed(&h->meta[cur].vstart) / kQcSpots;
+        r0 = bcast(g, r0);
+        // lane r: the queue chunk of range r0 + r (lane 0: cur itself)
+        uint32_t c = r == 0u ? cur : recall_range(h, q, r0 + r);
+        bool pass = false;
+        uint32_t nx = kEmpty;
+        if (c < h->max_chunks && ld_relaxed(&h->meta[c].size) == tag) {
+          pass = (ld_acquire(&h->meta[c].qcount) & 0xFFFFu) == kQcSpots;
+          nx = ld_acquire(&h->meta[c].next);
+          pass = pass && nx < kInstalling;
+        }
+        // lane r continues lane r - 1's chain only if that chunk links to it
+        const uint32_t prev_next = __shfl_sync(g.mask, nx, lane_of_rank(g.mask, r > 0u ? static_cast<int>(r) - 1 : 0));
+        const bool ok = pass && (r == 0u || prev_next == c);
+        const uint32_t stop = __ballot_sync(g.mask, !ok);
+        const uint32_t k = stop ? first_rank(g, stop) : n;   // lanes 0 .. k-1 are passed
+        if (k == 0u) break;
+        cur = __shfl_sync(g.mask, nx, lane_of_rank(g.mask, static_cast<int>(k) - 1));
       }
       if (cur == bp) return;
-      const uint32_t seen = atomicCAS(&q->back_ptr, bp, cur);
+      uint32_t seen = 0;
+      if (g.is_leader()) seen = atomicCAS(&q->back_ptr, bp, cur);
+      seen = bcast(g, seen);
       if (seen == bp) return;
       bp = seen;   // moved by someone else: walk on from there
     }
@@ -627,13 +653,18 @@ struct VlStore {
   }
 
   // Count update of m enqueued entries into chunk c (QueueChunk_impl.cuh:160-182).
-  // Returns true when this update completes the chunk's drain: the caller's
-  // group then runs on_empty.
-  __device__ static bool count_enqueued(HeapCore* h, ClassState* q, uint32_t c, uint32_t m) {
+  // Returns kFilled when this update fills the chunk (the caller's group then
+  // runs set_back) and kDrained when it completes the chunk's drain (then
+  // on_empty), in that order.
+  static constexpr uint32_t kDrained = 1u, kFilled = 2u;
+  __device__ static uint32_t count_enqueued(HeapCore* h, ClassState* q, uint32_t c, uint32_t m) {
     uint32_t add = (m << 16) + m;
     uint32_t old = atomicAdd(&h->meta[c].qcount, add);
-    if ((old & 0xFFFFu) + m == kQcSpots) set_back(h, q);
-    return old + add == kQcSpots;
+    return ((old & 0xFFFFu) + m == kQcSpots ? kFilled : 0u) | (old + add == kQcSpots ? kDrained : 0u);
+  }
+  __device__ static void after_enqueue(HeapCore* h, ClassState* q, const Group& g, uint32_t flags) {
+    if (flags & kFilled) set_back(h, q, g);
+    if (flags & kDrained) on_empty(h, q, g);
   }
 
   __device__ static bool count_removed(HeapCore* h, ClassState* q, uint32_t c, uint32_t m) {
@@ -739,9 +770,9 @@ struct VlStore {
       }
       __syncwarp(g.mask);
       __threadfence();
-      uint32_t drained = 0;
-      if (g.is_leader()) drained = count_enqueued(h, q, qc, j1 - j0) ? 1u : 0u;
-      if (bcast(g, drained)) on_empty(h, q, g);
+      uint32_t flags = 0;
+      if (g.is_leader()) flags = count_enqueued(h, q, qc, j1 - j0);
+      after_enqueue(h, q, g, bcast(g, flags));
     }
   }
 
@@ -767,9 +798,9 @@ struct VlStore {
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), v);
     __syncwarp(sg.mask);
     __threadfence();
-    uint32_t drained = 0;
-    if (sg.is_leader()) drained = count_enqueued(h, q, qc, static_cast<uint32_t>(sg.size)) ? 1u : 0u;
-    if (bcast(sg, drained)) on_empty(h, q, sg);
+    uint32_t flags = 0;
+    if (sg.is_leader()) flags = count_enqueued(h, q, qc, static_cast<uint32_t>(sg.size));
+    after_enqueue(h, q, sg, bcast(sg, flags));
   }
 
   __device__ static uint32_t consume_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos) {
@@ -807,7 +838,7 @@ struct VlStore {
     __threadfence();
     st_release(queue_slots(h, qc) + (b % kQcSpots), c);
     __threadfence();
-    if (count_enqueued(h, q, qc, 1u)) on_empty(h, q, self);
+    after_enqueue(h, q, self, count_enqueued(h, q, qc, 1u));
     return true;
   }
   struct Cursor { uint32_t chunk; };
