@@ -332,6 +332,27 @@ struct VaStore {
     uint32_t a = f & ~3u, stop = 0, range = kEmpty, qc = kEmpty;
     bool found = false;
     for (uint32_t r = 0, rounds = front_rounds(n); r < rounds && !found; ++r, a += 4u * n) {
+      // A queue chunk whose 2048 entries were all written and all removed
+      // (qcount: 0 present, 2048 enqueued) is passed whole, without reading
+      // its entries: after a burst the front may trail the live entries by
+      // hundreds of such chunks.
+      uint32_t skip = a;
+      if (g.is_leader()) {
+        for (uint32_t k = 0; k < 64u; ++k) {
+          const uint32_t rg = skip / kQcSpots, end = (rg + 1u) * kQcSpots;
+          if (static_cast<int32_t>(end - back) > 0) break;
+          const uint32_t c = ld_acquire(q->ring + vid(skip));
+          if (c >= kInstalling || ld_relaxed(&h->meta[c].vstart) / kQcSpots != rg) break;
+          if (ld_acquire(&h->meta[c].qcount) != kQcSpots) break;
+          skip = end;
+        }
+      }
+      a = bcast(g, skip);
+      if (static_cast<int32_t>(a - back) >= 0) {
+        stop = back;
+        found = true;
+        break;
+      }
       const uint32_t p = a + 4u * static_cast<uint32_t>(g.rank);
       uint4 e = make_uint4(0, 0, 0, 0);
       if (static_cast<int32_t>(p - back) < 0) {
@@ -353,18 +374,20 @@ struct VaStore {
     uint32_t cur = 0;
     if (g.is_leader()) cur = claim_front(q, f, stop);
     cur = bcast(g, cur);
-    // every queue chunk whose last entry lies in [cur, stop) is now behind the front
-    for (uint32_t end = cur - cur % kQcSpots + kQcSpots; static_cast<int32_t>(stop - end) >= 0; end += kQcSpots) {
-      uint32_t c = kEmpty;
-      if (g.is_leader()) c = atomicExch(q->ring + vid(end - 1u), kEmpty);
-      c = bcast(g, c);
+    // every queue chunk whose last entry lies in [cur, stop) is now behind the
+    // front: one per lane takes it out of the index, cleans its entries and
+    // returns it to the pool
+    const uint4 empty = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
+    for (uint32_t end0 = cur - cur % kQcSpots + kQcSpots; static_cast<int32_t>(stop - end0) >= 0;
+         end0 += n * kQcSpots) {
+      const uint32_t end = end0 + static_cast<uint32_t>(g.rank) * kQcSpots;
+      if (static_cast<int32_t>(stop - end) < 0) continue;
+      const uint32_t c = atomicExch(q->ring + vid(end - 1u), kEmpty);
       if (c >= kInstalling) continue;
       uint32_t* slots = queue_slots(h, c);
-      const uint4 empty = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
-      for (uint32_t i = 4u * static_cast<uint32_t>(g.rank); i < kQcSpots; i += 4u * n) st_v4(slots + i, empty);
-      __syncwarp(g.mask);
+      for (uint32_t i = 0; i < kQcSpots; i += 4u) st_v4(slots + i, empty);
       __threadfence();
-      if (g.is_leader()) reuse_put(h, &h->reuse[0], c);
+      reuse_put(h, &h->reuse[0], c);
     }
   }
 };
