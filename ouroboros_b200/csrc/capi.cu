@@ -287,6 +287,7 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
   if (e == cudaSuccess) e = cudaMemset(h->base + L.data_off, 0xFF, L.ring_off - L.data_off);
   const unsigned long long q_end = L.reuse_off + 2ull * kReuseSize * 4u;
   if (e == cudaSuccess) e = cudaMemset(h->base + L.ring_off, 0xFF, q_end - L.ring_off);
+  if (e == cudaSuccess && variant / 2 == 0) e = cudaMemset(h->base + L.seg_off, 0, kNumClasses * kRingSegs * 4ull);
   HeapCore core;
   std::memset(&core, 0, sizeof(core));
   core.variant = variant;
@@ -320,6 +321,7 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
       q.ring = reinterpret_cast<uint32_t*>(h->base + L.ring_off) + static_cast<size_t>(c) * kRingSize;
       q.ring_mask = kRingSize - 1u;
       q.page_cap = kRingSize;
+      q.seg = reinterpret_cast<uint32_t*>(h->base + L.seg_off) + static_cast<size_t>(c) * kRingSegs;
     } else if (kind == 1) {
       q.ring = reinterpret_cast<uint32_t*>(h->base + L.vq_off) + static_cast<size_t>(c) * kVqSize;
       q.ring_mask = kVqSize - 1u;

@@ -49,6 +49,7 @@ struct alignas(128) ClassState {
   uint32_t page_cap;
   uint32_t clean_on_recycle;      // chunk queues: queue chunks hold kTomb entries when drained
   uint32_t* skip;                 // linked: index of recently linked queue chunks
+  uint32_t* seg;                  // standard chunk queues: removed entries per 2048-entry ring segment
 };
 
 struct alignas(128) ReuseQueue {
@@ -121,7 +122,7 @@ struct Layout {
   unsigned long long ref_queue_bytes;
   unsigned long long ref_total_required;
   unsigned long long max_chunks;
-  unsigned long long meta_off, data_off, ring_off, vq_off, skip_off, reuse_off;
+  unsigned long long meta_off, data_off, ring_off, vq_off, skip_off, reuse_off, seg_off;
   unsigned long long alloc_bytes;
 };
 
@@ -152,6 +153,8 @@ __host__ inline bool compute_layout(int kind, unsigned long long heap_bytes, Lay
   if (kind == 2) off += (unsigned long long)kNumClasses * kSkipSlots * 4u;
   L->reuse_off = off;
   off += 2ull * kReuseSize * 4u;
+  L->seg_off = off;
+  if (kind == 0) off += (unsigned long long)kNumClasses * kRingSegs * 4u;
   L->alloc_bytes = align_up(off, kChunkBytes) + kChunkBytes;   // + slack to 8 KiB-align the base
   return true;
 }

@@ -131,9 +131,23 @@ struct FlatStore {
   struct Cursor { uint32_t unused; };
   __device__ static Cursor cursor(ClassState*) { return Cursor{0}; }
   __device__ static uint32_t peek(HeapCore* h, ClassState* q, uint32_t pos, Cursor&) { return ld_acquire(slot(q, pos)); }
-  __device__ static void remove(HeapCore* h, ClassState* q, uint32_t pos) { st_relaxed(slot(q, pos), kTomb); }
+  // The removal is counted per 2048-entry segment of the ring after the
+  // tombstone is written, so a count never runs ahead of the tombstones.
+  __device__ static uint32_t* seg_count(ClassState* q, uint32_t pos) {
+    return q->seg + ((pos / 2048u) & (kRingSegs - 1u));
+  }
+  __device__ static void remove(HeapCore* h, ClassState* q, uint32_t pos) {
+    st_relaxed(slot(q, pos), kTomb);
+    __threadfence();
+    atomicAdd(seg_count(q, pos), 1u);
+  }
 
   // Move the front past removed entries, freeing their slots for the next lap.
+  // A segment whose 2048 entries all lie before the back and were all removed
+  // (its count says 2048) is passed without reading its entries.  Passed
+  // slots go back to kEmpty; a segment whose end the front passes has its
+  // count lowered by 2048 for the next lap (lowered, not reset, so that a
+  // count still in flight is kept).
   __device__ static void advance_front(HeapCore* h, ClassState* q, const Group& g) {
     uint32_t f = 0, back = 0;
     if (g.is_leader()) {
@@ -147,6 +161,21 @@ struct FlatStore {
     uint32_t a = f & ~3u, stop = 0;
     bool found = false;
     for (uint32_t r = 0, rounds = front_rounds(n); r < rounds && !found; ++r, a += 4u * n) {
+      uint32_t skip = a;
+      if (g.is_leader() && q->seg) {
+        for (uint32_t k = 0; k < 64u; ++k) {
+          const uint32_t end = (skip / 2048u + 1u) * 2048u;
+          if (static_cast<int32_t>(end - back) > 0) break;
+          if (ld_acquire(seg_count(q, skip)) != 2048u) break;
+          skip = end;
+        }
+      }
+      a = bcast(g, skip);
+      if (static_cast<int32_t>(a - back) >= 0) {
+        stop = back;
+        found = true;
+        break;
+      }
       const uint32_t p = a + 4u * static_cast<uint32_t>(g.rank);
       // ring positions are 4-aligned here and the ring size is a multiple of 4
       const uint4 e = static_cast<int32_t>(p - back) < 0 ? ld_relaxed_v4(slot(q, p)) : make_uint4(0, 0, 0, 0);
@@ -161,8 +190,30 @@ struct FlatStore {
     uint32_t cur = 0;
     if (g.is_leader()) cur = claim_front(q, f, stop);
     cur = bcast(g, cur);
-    for (uint32_t p = cur + static_cast<uint32_t>(g.rank); p != stop && static_cast<int32_t>(p - stop) < 0; p += n)
-      st_relaxed(slot(q, p), kEmpty);
+    if (!q->seg) {
+      for (uint32_t p = cur + static_cast<uint32_t>(g.rank); p != stop && static_cast<int32_t>(p - stop) < 0; p += n)
+        st_relaxed(slot(q, p), kEmpty);
+      return;
+    }
+    // [cur, stop): the partial segments at either end slot by slot, whole
+    // segments one per lane with 16-byte stores
+    const uint32_t s0 = (cur + 2047u) / 2048u * 2048u, s1 = stop / 2048u * 2048u;
+    if (static_cast<int32_t>(s1 - s0) <= 0) {
+      for (uint32_t p = cur + static_cast<uint32_t>(g.rank); static_cast<int32_t>(p - stop) < 0; p += n)
+        st_relaxed(slot(q, p), kEmpty);
+    } else {
+      for (uint32_t p = cur + static_cast<uint32_t>(g.rank); static_cast<int32_t>(p - s0) < 0; p += n)
+        st_relaxed(slot(q, p), kEmpty);
+      for (uint32_t p = s1 + static_cast<uint32_t>(g.rank); static_cast<int32_t>(p - stop) < 0; p += n)
+        st_relaxed(slot(q, p), kEmpty);
+      const uint4 empty = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
+      for (uint32_t b0 = s0 + static_cast<uint32_t>(g.rank) * 2048u; static_cast<int32_t>(s1 - b0) > 0; b0 += n * 2048u)
+        for (uint32_t i = 0; i < 2048u; i += 4u) st_v4(slot(q, b0 + i), empty);
+    }
+    // segments whose end the front passed: their count starts the next lap
+    for (uint32_t end = (cur / 2048u + 1u) * 2048u + static_cast<uint32_t>(g.rank) * 2048u;
+         static_cast<int32_t>(stop - end) >= 0; end += n * 2048u)
+      atomicSub(seg_count(q, end - 1u), 2048u);
   }
 };
 
