@@ -383,13 +383,12 @@ __device__ __forceinline__ uint32_t group_exclusive_sum(const Group& g, uint32_t
   return incl - v;
 }
 
-// A group that needs several chunks' worth of pages (more lanes than a chunk
-// has pages) takes one run of that many positions from the scan cursor and
-// works it in parallel: lane r examines position r of the run (entry, page
-// size, free count), reserves on its chunk what the group still needs after
-// the lanes below it, the pages are claimed chunk by chunk and the takers of a
-// chunk's last pages remove its entry.  Whatever the run could not serve is
-// left to the probe loop.
+// A group takes one run of ceil(lanes / pages-per-chunk) positions from the
+// scan cursor and works it in parallel: lane r examines position r of the run
+// (entry, page size, free count), reserves on its chunk what the group still
+// needs after the lanes below it, the pages are claimed chunk by chunk and the
+// takers of a chunk's last pages remove its entry.  Whatever the run could not
+// serve is left to the probe loop.
 template <class Store>
 __device__ void chunk_alloc_run(HeapCore* h, ClassState* q, const Group& s, typename Store::Cursor& cur,
                                 uint32_t run, bool& served, uint32_t& page, uint32_t& chunk) {
@@ -469,8 +468,11 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
   typename Store::Cursor cur = Store::cursor(q);
   uint32_t need = static_cast<uint32_t>(s.size);
   {
+    // A group starts with a run from the cursor, which spreads concurrent
+    // groups over the chunks; a lone lane starts at the front as the
+    // reference does.
     const uint32_t run = (need + q->ppc - 1u) / q->ppc;
-    if (run > 1u) {
+    if (s.size > 1) {
       chunk_alloc_run<Store>(h, q, s, cur, run, served, page, chunk);
       // the whole group stays in the probe loop, served lanes included: its
       // sweeps cover one position per lane of the group, not of the rest
