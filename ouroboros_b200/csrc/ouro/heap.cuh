@@ -204,11 +204,14 @@ __device__ inline void reuse_put(HeapCore* h, ReuseQueue* r, uint32_t chunk) {
 
 // ---------------------------------------------------- chunk allocation
 // Ouroboros.cuh:108-136 / 200-229 allocateChunk, for a whole group: up to k
-// chunks (k <= group size), reuse queue first, then the bump pointer.  Lane
-// with rank i < result holds its chunk index in *mine.  A chunk is valid when
-// index + factor < max_chunks (the reference's bound).
-__device__ inline uint32_t alloc_chunks(HeapCore* h, const Group& g, uint32_t k, uint32_t inst, bool queue_chunk,
-                                        uint32_t* mine) {
+// chunks (k <= R x group size) with one reservation, reuse queue first, then
+// the bump pointer.  Chunk i of the k goes to the lane of rank i mod n, in
+// mine[i / n]; chunks i < result are valid (a reuse slot that timed out
+// leaves kEmpty).  A chunk is valid when index + factor < max_chunks (the
+// reference's bound).
+template <int R>
+__device__ inline uint32_t alloc_chunk_rounds(HeapCore* h, const Group& g, uint32_t k, uint32_t inst, bool queue_chunk,
+                                              uint32_t (&mine)[R]) {
   const uint32_t factor = queue_chunk ? 1u : instance_factor(inst);
   ReuseQueue* r = (inst != 0u && queue_chunk) ? &h->reuse[0] : &h->reuse[inst];
   uint32_t from_reuse = 0, rpos = 0;
@@ -221,20 +224,32 @@ __device__ inline uint32_t alloc_chunks(HeapCore* h, const Group& g, uint32_t k,
   from_reuse = bcast(g, from_reuse);
   rpos = bcast(g, rpos);
   first = bcast64(g, first);
-  uint32_t got = from_reuse;
-  const uint32_t r_ = static_cast<uint32_t>(g.rank);
-  uint32_t c = kEmpty;
-  if (r_ < from_reuse) {
-    c = reuse_read(h, r, rpos + r_);
-  } else if (r_ < k) {
-    unsigned long long idx = first + (unsigned long long)(r_ - from_reuse) * factor;
-    if (idx + factor < h->max_chunks) c = static_cast<uint32_t>(idx);
+  const uint32_t n = static_cast<uint32_t>(g.size);
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    const uint32_t i = static_cast<uint32_t>(j) * n + static_cast<uint32_t>(g.rank);
+    uint32_t c = kEmpty;
+    if (i < from_reuse) {
+      c = reuse_read(h, r, rpos + i);
+    } else if (i < k) {
+      unsigned long long idx = first + (unsigned long long)(i - from_reuse) * factor;
+      if (idx + factor < h->max_chunks) c = static_cast<uint32_t>(idx);
+    }
+    mine[j] = c;
   }
   // bumped chunks are valid as a prefix of their range
   unsigned long long avail = h->max_chunks > first + factor ? (h->max_chunks - first - 1u) / factor : 0u;
   uint32_t bumped = k - from_reuse;
-  got += avail < bumped ? static_cast<uint32_t>(avail) : bumped;
-  *mine = c;
+  return from_reuse + (avail < bumped ? static_cast<uint32_t>(avail) : bumped);
+}
+
+// One chunk per lane (k <= group size): lane of rank i < result holds its
+// chunk in *mine.
+__device__ inline uint32_t alloc_chunks(HeapCore* h, const Group& g, uint32_t k, uint32_t inst, bool queue_chunk,
+                                        uint32_t* mine) {
+  uint32_t m[1];
+  const uint32_t got = alloc_chunk_rounds<1>(h, g, k, inst, queue_chunk, m);
+  *mine = m[0];
   return got;
 }
 

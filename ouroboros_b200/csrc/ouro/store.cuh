@@ -750,57 +750,72 @@ struct VlStore {
   // A producer at the start of a queue chunk links the next one
   // (QueueChunk_impl.cuh:144-158).  A link needs its predecessor, so linking
   // is a chain.  When producers already hold positions several queue chunks
-  // ahead (a burst), the group links up to one chunk per lane at once: one
-  // allocation, headers and links written in parallel, one CAS to attach the
-  // piece, and index entries written right after, so that waiting producers
-  // find their chunk in the index instead of walking.  The producer at the
-  // start of the piece's last range continues the chain.  The piece is only
-  // ever attached to c, whose range the caller holds a position of: c cannot
-  // drain meanwhile.  (A chunk the caller does not hold may be drained,
-  // recycled and reused with an empty link, and a piece attached there would
-  // duplicate ranges of the live chain.)  A lone producer is never more than
-  // one chunk ahead, so it links exactly one chunk, as the reference does.
-  // c holds the range starting at pos.  Collective over g.
+  // ahead (a burst), the group links a piece of up to kPieceRounds chunks per
+  // lane at once: one reservation of chunks, headers and links written in
+  // parallel, one CAS to attach the piece, and index entries written right
+  // after, so that waiting producers find their chunk in the index instead of
+  // walking.  The producer at the start of the piece's last range continues
+  // the chain, so a burst of B queue chunks waits for B / (kPieceRounds x 32)
+  // links in a row.  The piece is only ever attached to c, whose range the
+  // caller holds a position of: c cannot drain meanwhile.  (A chunk the
+  // caller does not hold may be drained, recycled and reused with an empty
+  // link, and a piece attached there would duplicate ranges of the live
+  // chain.)  A lone producer is never more than one chunk ahead, so it links
+  // exactly one chunk, as the reference does.  c holds the range starting at
+  // pos.  Collective over g.
+  static constexpr int kPieceRounds = 4;
   __device__ static void preallocate(HeapCore* h, ClassState* q, const Group& g, uint32_t c, uint32_t pos) {
     uint32_t* link = &h->meta[c].next;
+    const uint32_t n = static_cast<uint32_t>(g.size), r = static_cast<uint32_t>(g.rank);
     uint32_t ahead = 0;
     if (g.is_leader() && ld_relaxed(link) == kEmpty) {
       const uint32_t back = ld_relaxed(&q->back.v);
       ahead = static_cast<int32_t>(back - pos) > static_cast<int32_t>(2u * kQcSpots)
                   ? (back - pos) / kQcSpots - 1u : 1u;
-      if (ahead > static_cast<uint32_t>(g.size)) ahead = static_cast<uint32_t>(g.size);
+      if (ahead > kPieceRounds * n) ahead = kPieceRounds * n;
     }
     ahead = bcast(g, ahead);
     if (!ahead) return;
-    const uint32_t n = static_cast<uint32_t>(g.size), r = static_cast<uint32_t>(g.rank);
-    uint32_t mine = kEmpty;
-    const uint32_t got = alloc_chunks(h, g, ahead, q->inst, true, &mine);
-    const bool have = r < got && mine != kEmpty;
-    const uint32_t miss = __ballot_sync(g.mask, !have);
-    const uint32_t L = miss ? first_rank(g, miss) : n;
-    const uint32_t succ = __shfl_sync(g.mask, mine, lane_of_rank(g.mask, r + 1u < n ? static_cast<int>(r) + 1
-                                                                                   : static_cast<int>(r)));
-    const uint32_t vstart = pos + (r + 1u) * kQcSpots;
-    if (r < L) {
-      init_queue_chunk(h, mine, vstart, queue_tag(q));
-      if (r + 1u < L) st_relaxed(&h->meta[mine].next, succ);
-      __threadfence();
-    } else if (have) {
-      reuse_put(h, &h->reuse[0], mine);   // behind a hole: not part of the piece
+    uint32_t mine[kPieceRounds];
+    const uint32_t got = alloc_chunk_rounds<kPieceRounds>(h, g, ahead, q->inst, true, mine);
+    // the piece is the prefix of chunks up to the first one missing
+    uint32_t hole = ahead;
+#pragma unroll
+    for (int j = 0; j < kPieceRounds; ++j) {
+      const uint32_t i = static_cast<uint32_t>(j) * n + r;
+      if (i < ahead && (i >= got || mine[j] == kEmpty) && i < hole) hole = i;
     }
+    const uint32_t L = __reduce_min_sync(g.mask, hole);
+    const int next_lane = lane_of_rank(g.mask, r + 1u < n ? static_cast<int>(r) + 1 : static_cast<int>(r));
+#pragma unroll
+    for (int j = 0; j < kPieceRounds; ++j) {
+      const uint32_t i = static_cast<uint32_t>(j) * n + r;
+      const uint32_t succ_same = __shfl_sync(g.mask, mine[j], next_lane);
+      const uint32_t succ_next = __shfl_sync(g.mask, mine[j + 1 < kPieceRounds ? j + 1 : j], g.leader);
+      if (i < L) {
+        init_queue_chunk(h, mine[j], pos + (i + 1u) * kQcSpots, queue_tag(q));
+        if (i + 1u < L) st_relaxed(&h->meta[mine[j]].next, r + 1u < n ? succ_same : succ_next);
+      } else if (i < got && mine[j] != kEmpty) {
+        reuse_put(h, &h->reuse[0], mine[j]);   // behind a hole: not part of the piece
+      }
+    }
+    __threadfence();
     __syncwarp(g.mask);
     if (L == 0u) return;
-    const uint32_t piece = __shfl_sync(g.mask, mine, g.leader);
+    const uint32_t piece = __shfl_sync(g.mask, mine[0], g.leader);
     uint32_t ok = 0;
     if (g.is_leader()) ok = atomicCAS(link, kEmpty, piece) == kEmpty ? 1u : 0u;
     ok = bcast(g, ok);
-    if (r < L) {
+#pragma unroll
+    for (int j = 0; j < kPieceRounds; ++j) {
+      const uint32_t i = static_cast<uint32_t>(j) * n + r;
+      if (i >= L) continue;
       if (ok) {
-        remember(h, q, mine, vstart);
+        remember(h, q, mine[j], pos + (i + 1u) * kQcSpots);
       } else {   // someone else linked it: the piece goes back, untagged
-        st_relaxed(&h->meta[mine].size, 0u);
+        st_relaxed(&h->meta[mine[j]].size, 0u);
         __threadfence();
-        reuse_put(h, &h->reuse[0], mine);
+        reuse_put(h, &h->reuse[0], mine[j]);
       }
     }
   }
