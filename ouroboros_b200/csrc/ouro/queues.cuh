@@ -257,22 +257,25 @@ __device__ void help_front(HeapCore* h, ClassState* q, const Group& g) {
 }
 
 // Remove the entry of an exhausted chunk (the DEQUEUE_CHUNK mode of
-// ChunkQueue_impl.cuh:128-137).  Called by one lane; returns true when it
-// removed the entry, after which its group should help the front.
+// ChunkQueue_impl.cuh:128-137).  Called by one lane; returns kRemoved when it
+// removed the entry, after which its group should help the front, plus
+// kDrainedQc when the removal drained a queue chunk, after which its group
+// runs Store::after_drain.
+constexpr uint32_t kRemoved = 1u, kDrainedQc = 2u;
 template <class Store>
-__device__ bool chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos) {
+__device__ uint32_t chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos) {
   uint32_t* qp = &h->meta[c].queue_pos;
   uint32_t it = 0;
   while (ld_relaxed(qp) == kPending) {
-    if (it >= 4096u) return false;
+    if (it >= 4096u) return 0u;
     backoff(it);
   }
-  if (atomicCAS(qp, pos, kEmpty) != pos) return false;   // someone else removed or moved it
-  Store::remove(h, q, pos);
+  if (atomicCAS(qp, pos, kEmpty) != pos) return 0u;   // someone else removed or moved it
+  const bool drained = Store::remove(h, q, pos);
   atomicSub(&q->entries.v, 1);
   __threadfence();
   if (ld_relaxed(&h->meta[c].count) > 0) ensure_enqueued<Store>(h, q, c);
-  return true;
+  return kRemoved | (drained ? kDrainedQc : 0u);
 }
 
 // Cooperative claim of `got` free pages of chunk c for the unserved lanes of
@@ -434,8 +437,9 @@ __device__ void chunk_alloc_run(HeapCore* h, ClassState* q, const Group& s, type
     else claim_pages<1u>(h, s, c, k, served, page);
     if (served && !was) chunk = c;
   }
-  const bool removed = last && chunk_dequeue<Store>(h, q, v, pos);
-  if (__ballot_sync(s.mask, removed)) help_front<Store>(h, q, s);
+  const uint32_t rf = last ? chunk_dequeue<Store>(h, q, v, pos) : 0u;
+  if (__ballot_sync(s.mask, (rf & kDrainedQc) != 0u)) Store::after_drain(h, q, s);
+  if (__ballot_sync(s.mask, rf != 0u)) help_front<Store>(h, q, s);
 }
 
 // ChunkQueue_impl.cuh:82-148 allocPage, for a group.  The first probe is the
@@ -560,10 +564,12 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
       if (served && !before) chunk = c;
       uint32_t removed = 0;
       if (s.is_leader()) {
-        if (last) removed = chunk_dequeue<Store>(h, q, c, pos) ? 1u : 0u;
+        if (last) removed = chunk_dequeue<Store>(h, q, c, pos);
         ++pos;
       }
-      if (bcast(s, removed)) help_front<Store>(h, q, s);
+      removed = bcast(s, removed);
+      if (removed & kDrainedQc) Store::after_drain(h, q, s);
+      if (removed) help_front<Store>(h, q, s);
 #ifdef OURO_SCAN_STATS
       t_deq += clock64() - t0;
 #endif
@@ -658,7 +664,7 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
   if (wg.is_leader()) atomicOr(&m->mask[page >> 5], bits);
   __syncwarp(cg.mask);
   __threadfence();
-  uint32_t flashed = 0, help = 0, enq = 0;
+  uint32_t flashed = 0, help = 0, enq = 0, drained = 0;
   if (cg.is_leader()) {
     const int32_t n = cg.size;
     int32_t old = atomicAdd(&m->count, n);
@@ -679,7 +685,7 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
           uint32_t qp, it = 0;
           while ((qp = ld_relaxed(&m->queue_pos)) == kPending && it < 4096u) backoff(it);
           if (qp != kPending && qp != kEmpty && atomicCAS(&m->queue_pos, qp, kEmpty) == qp) {
-            Store::remove(h, q, qp);
+            drained = Store::remove(h, q, qp) ? 1u : 0u;
             atomicSub(&q->entries.v, 1);
             flashed = 2u;
           } else {
@@ -697,6 +703,7 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
   if (enq) chunk_enqueue_group<Store>(h, q, make_group(em), c);
   flashed = __shfl_sync(cg.mask, flashed, cg.leader);
   help = __shfl_sync(cg.mask, help, cg.leader);
+  if (__shfl_sync(cg.mask, drained, cg.leader)) Store::after_drain(h, q, cg);
   if (flashed == 2u || help) help_front<Store>(h, q, cg);
   __syncwarp(g.mask);
   __threadfence();

@@ -136,11 +136,13 @@ struct FlatStore {
   __device__ static uint32_t* seg_count(ClassState* q, uint32_t pos) {
     return q->seg + ((pos / 2048u) & (kRingSegs - 1u));
   }
-  __device__ static void remove(HeapCore* h, ClassState* q, uint32_t pos) {
+  __device__ static bool remove(HeapCore* h, ClassState* q, uint32_t pos) {
     st_relaxed(slot(q, pos), kTomb);
     __threadfence();
     atomicAdd(seg_count(q, pos), 1u);
+    return false;
   }
+  __device__ static void after_drain(HeapCore*, ClassState*, const Group&) {}
 
   // Move the front past removed entries, freeing their slots for the next lap.
   // A segment whose 2048 entries all lie before the back and were all removed
@@ -359,12 +361,14 @@ struct VaStore {
     if (ld_relaxed(&h->meta[qc].vstart) / kQcSpots != pos / kQcSpots) return kTomb;
     return ld_acquire(queue_slots(h, qc) + (pos % kQcSpots));
   }
-  __device__ static void remove(HeapCore* h, ClassState* q, uint32_t pos) {
+  __device__ static bool remove(HeapCore* h, ClassState* q, uint32_t pos) {
     uint32_t qc = ld_acquire(q->ring + vid(pos));
-    if (qc >= kInstalling) return;
+    if (qc >= kInstalling) return false;
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
     atomicSub(&h->meta[qc].qcount, 1u << 16);
+    return false;   // queue chunks return to the pool from the front
   }
+  __device__ static void after_drain(HeapCore*, ClassState*, const Group&) {}
   // Front moves over removed entries; passing the last entry of a queue chunk
   // returns that chunk to the pool (ChunkQueueVA_impl.cuh:144-156).  Each lane
   // keeps the queue chunk of its own positions and looks the next one up when
@@ -953,13 +957,17 @@ struct VlStore {
     cur.chunk = qc;
     return ld_acquire(queue_slots(h, qc) + (pos % kQcSpots));
   }
-  __device__ static void remove(HeapCore* h, ClassState* q, uint32_t pos) {
+  // Returns true when this removal drained the queue chunk: the caller's
+  // group then runs after_drain (on_empty), so that front_ptr moves with a
+  // whole group's walk rather than one lane's.
+  __device__ static bool remove(HeapCore* h, ClassState* q, uint32_t pos) {
     uint32_t qc = locate_live(h, q, &q->front_ptr, pos);
-    if (qc == kEmpty || qc == kBehind) return;
+    if (qc == kEmpty || qc == kBehind) return false;
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
     __threadfence();
-    if (count_removed(h, q, qc, 1u)) on_empty(h, q, make_group(1u << lane_id()));
+    return count_removed(h, q, qc, 1u);
   }
+  __device__ static void after_drain(HeapCore* h, ClassState* q, const Group& g) { on_empty(h, q, g); }
   // Front moves over removed entries.  The leader walks the chain: per round
   // the group's positions span at most two queue chunks (4 x 32 < 2048), the
   // current one and its successor.  Drained queue chunks leave the chain
