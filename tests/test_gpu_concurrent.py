@@ -154,6 +154,36 @@ def test_burst_grows_past_one_queue_chunk(v, size):
         assert st["flags"] == 0 and st["timeouts"] == 0, st
 
 
+@pytest.mark.parametrize("v,reps", [("C", 72), ("VAC", 140), ("VLC", 40)])
+def test_chunk_queue_wraps_around(v, reps):
+    # Bursts of 2^20 requests of 2 KiB: every free phase re-enqueues 262,144
+    # chunks, so the back of the class's queue moves 262,144 positions per
+    # burst.  The standard ring (2^23 entries) wraps every 32 bursts and the
+    # virtualized-array index (16,384 queue chunks of 2048 entries) every 128;
+    # the front passes fully removed ring segments and queue chunks on their
+    # removal counts, which must start every lap clean.  Checked rounds along
+    # the way: every page handed out once, every wait ended.
+    n, size, cls = 1 << 20, 2048, 7
+    with ob.Ouroboros(v, 4 * GiB) as heap:
+        ptrs = _ptrs(n)
+        back0 = int(heap.state()[7 + 12 * cls + 4])
+        for r in range(reps):
+            if r % 16 == 15 or r == reps - 1:
+                rep, nulls, bad = _round(heap, ptrs, n, size, seed=r)
+                assert nulls == 0 and bad == 0, (r, nulls, bad)
+                assert rep["overlaps"] == 0 and rep["misaligned"] == 0 and rep["out_of_heap"] == 0, (r, rep)
+            else:
+                heap.alloc(ptrs, n, size)
+                heap.free(ptrs, n)
+        torch.cuda.synchronize()
+        moved = int(heap.state()[7 + 12 * cls + 4]) - back0
+        laps = {"C": 1 << 23, "VAC": 16384 * 2048, "VLC": 0}[v]
+        assert moved > laps, (moved, laps)
+        st = heap.status()
+        assert st["flags"] == 0 and st["timeouts"] == 0, st
+        _idle(heap, v)
+
+
 @pytest.mark.parametrize("v", ob.VARIANTS)
 def test_free_resources_accounting(v):
     # free bytes = free pages x page size + chunks never handed out or pooled
