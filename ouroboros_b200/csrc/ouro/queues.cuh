@@ -428,14 +428,51 @@ __device__ void chunk_alloc_run(HeapCore* h, ClassState* q, const Group& s, type
     }
     last = got > 0u && old <= static_cast<int32_t>(want);
   }
-  for (uint32_t m = __ballot_sync(s.mask, got > 0u); m; m &= m - 1u) {
-    const int src = __ffs(m) - 1;
-    const uint32_t c = __shfl_sync(s.mask, v, src);
-    const uint32_t k = __shfl_sync(s.mask, got, src);
-    const bool was = served;
-    if (q->inst == 0u) claim_pages<16u>(h, s, c, k, served, page);
-    else claim_pages<1u>(h, s, c, k, served, page);
-    if (served && !was) chunk = c;
+  if (run > 1u) {
+    // More than one chunk: a chunk then has at most 16 pages, all in mask
+    // word 0, so every lane that reserved pages claims its own chunk's bits
+    // (lowest first) at the same time, and the won pages go to the lanes in
+    // rank order by a prefix sum over them.
+    uint32_t won = 0;
+    if (got) {
+      uint32_t* mw = &h->meta[v].mask[0];
+      uint32_t remaining = got;
+      for (uint32_t attempt = 0; attempt < 64u && remaining; ++attempt) {
+        const uint32_t w = ld_relaxed(mw);
+        const uint32_t avail = static_cast<uint32_t>(__popc(w));
+        const uint32_t take = avail < remaining ? avail : remaining;
+        if (!take) continue;
+        const uint32_t p = __fns(w, 0u, static_cast<int>(take));   // the take-th lowest set bit
+        const uint32_t picked = w & (p == 31u ? ~0u : ((2u << p) - 1u));
+        const uint32_t wonnow = picked & atomicAnd(mw, ~picked);
+        won |= wonnow;
+        remaining -= static_cast<uint32_t>(__popc(wonnow));
+      }
+      if (remaining) set_status(h, kErrCorrupt);   // count promised pages the mask did not show
+    }
+    const uint32_t wcnt = static_cast<uint32_t>(__popc(won));
+    const uint32_t first = group_exclusive_sum(s, wcnt);
+    for (uint32_t m = __ballot_sync(s.mask, won != 0u); m; m &= m - 1u) {
+      const int src = __ffs(m) - 1;
+      const uint32_t c = __shfl_sync(s.mask, v, src);
+      const uint32_t wb = __shfl_sync(s.mask, won, src);
+      const uint32_t f0 = __shfl_sync(s.mask, first, src);
+      if (r >= f0 && r < f0 + static_cast<uint32_t>(__popc(wb))) {
+        page = __fns(wb, 0u, static_cast<int>(r - f0 + 1u));
+        chunk = c;
+        served = true;
+      }
+    }
+  } else {
+    for (uint32_t m = __ballot_sync(s.mask, got > 0u); m; m &= m - 1u) {
+      const int src = __ffs(m) - 1;
+      const uint32_t c = __shfl_sync(s.mask, v, src);
+      const uint32_t k = __shfl_sync(s.mask, got, src);
+      const bool was = served;
+      if (q->inst == 0u) claim_pages<16u>(h, s, c, k, served, page);
+      else claim_pages<1u>(h, s, c, k, served, page);
+      if (served && !was) chunk = c;
+    }
   }
   const uint32_t rf = last ? chunk_dequeue<Store>(h, q, v, pos) : 0u;
   if (__ballot_sync(s.mask, (rf & kDrainedQc) != 0u)) Store::after_drain(h, q, s);
