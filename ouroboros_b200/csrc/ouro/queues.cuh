@@ -388,10 +388,11 @@ __device__ __forceinline__ uint32_t group_exclusive_sum(const Group& g, uint32_t
 
 // A group takes one run of ceil(lanes / pages-per-chunk) positions from the
 // scan cursor and works it in parallel: lane r examines position r of the run
-// (entry, page size, free count), reserves on its chunk what the group still
-// needs after the lanes below it, the pages are claimed chunk by chunk and the
-// takers of a chunk's last pages remove its entry.  Whatever the run could not
-// serve is left to the probe loop.
+// (entry, page size, free count) and reserves on its chunk what the group
+// still needs after the lanes below it; the pages are claimed (each lane on
+// its own chunk when the run covers several, the group together when it is
+// one chunk) and the takers of a chunk's last pages remove its entry.
+// Whatever the run could not serve is left to the probe loop.
 template <class Store>
 __device__ void chunk_alloc_run(HeapCore* h, ClassState* q, const Group& s, typename Store::Cursor& cur,
                                 uint32_t run, bool& served, uint32_t& page, uint32_t& chunk) {
