@@ -596,68 +596,112 @@ struct VlStore {
   }
 
   // From chunk fp on, the queue chunks that are drained (all 2048 entries
-  // taken) and linked to a successor.  Lane r looks up the chunk of range
-  // (fp's range + r) in the index and checks that it is the successor of
-  // rank r-1's chunk, so a round covers up to one chunk per lane; an index
-  // miss ends the round early.  Returns how many chunks can be passed and
-  // moves *fp to the first one that cannot.  Collective over g.
+  // taken) and linked to a successor.  Index i = u x n + r (u = 0, 1: two
+  // chunks per lane and round) looks up the chunk of range (fp's range + i)
+  // in the index and checks that it is the successor of index i-1's chunk, so
+  // a round covers up to two chunks per lane; an index miss ends the round
+  // early.  Returns how many chunks can be passed and moves *fp to the first
+  // one that cannot.  Collective over g.
   __device__ static uint32_t walk_drained(HeapCore* h, ClassState* q, const Group& g, uint32_t* fp_io) {
     const uint32_t n = static_cast<uint32_t>(g.size), r = static_cast<uint32_t>(g.rank);
+    const int prev_lane = lane_of_rank(g.mask, r == 0u ? static_cast<int>(n) - 1 : static_cast<int>(r) - 1);
     uint32_t fp = *fp_io, passed = 0;
     uint32_t range = ld_relaxed(&h->meta[fp].vstart) / kQcSpots;
     for (uint32_t round = 0; round < (1u << 16); ++round) {
-      const uint32_t c = r == 0u ? fp : recall_range(h, q, range + r);
-      uint32_t cnt = 0, nx = kEmpty;
-      if (c != kEmpty) {
-        cnt = ld_acquire(&h->meta[c].qcount);
-        nx = ld_acquire(&h->meta[c].next);
+      uint32_t c[2], cnt[2] = {0u, 0u}, nx[2] = {kEmpty, kEmpty};
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const uint32_t i = static_cast<uint32_t>(u) * n + r;
+        c[u] = i == 0u ? fp : recall_range(h, q, range + i);
       }
-      const uint32_t prev_nx = __shfl_sync(g.mask, nx, lane_of_rank(g.mask, r == 0u ? 0 : static_cast<int>(r) - 1));
-      const bool linked = r == 0u || (c != kEmpty && c == prev_nx);
-      const bool pass = linked && cnt == kQcSpots && nx < kInstalling;
-      const uint32_t stop_m = __ballot_sync(g.mask, !pass);
-      const uint32_t k = stop_m ? first_rank(g, stop_m) : n;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        if (c[u] != kEmpty) {
+          cnt[u] = ld_acquire(&h->meta[c[u]].qcount);
+          nx[u] = ld_acquire(&h->meta[c[u]].next);
+        }
+      }
+      bool linked[2], pass[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const uint32_t i = static_cast<uint32_t>(u) * n + r;
+        const uint32_t same = __shfl_sync(g.mask, nx[u], prev_lane);          // index i-1 when r > 0
+        const uint32_t wrap = __shfl_sync(g.mask, nx[u > 0 ? u - 1 : 0], prev_lane);   // index i-1 when r == 0
+        const uint32_t prev = r > 0u ? same : wrap;
+        linked[u] = i == 0u || (c[u] != kEmpty && c[u] == prev);
+        pass[u] = linked[u] && cnt[u] == kQcSpots && nx[u] < kInstalling;
+      }
+      const uint32_t s0 = __ballot_sync(g.mask, !pass[0]), s1 = __ballot_sync(g.mask, !pass[1]);
+      const uint32_t k = s0 ? first_rank(g, s0) : (s1 ? n + first_rank(g, s1) : 2u * n);
       if (k == 0u) break;
-      fp = __shfl_sync(g.mask, nx, lane_of_rank(g.mask, static_cast<int>(k) - 1));
+      const int last = lane_of_rank(g.mask, static_cast<int>((k - 1u) % n));
+      const uint32_t a0 = __shfl_sync(g.mask, nx[0], last), a1 = __shfl_sync(g.mask, nx[1], last);
+      fp = (k - 1u) / n == 0u ? a0 : a1;
       passed += k;
       range += k;
-      if (k < n && __shfl_sync(g.mask, linked ? 1u : 0u, lane_of_rank(g.mask, static_cast<int>(k)))) break;
+      if (k < 2u * n) {
+        // stopped at a chunk that is linked but not passable: the walk ends;
+        // stopped at an index miss: the next round starts from the real link
+        const int at = lane_of_rank(g.mask, static_cast<int>(k % n));
+        const uint32_t l0 = __shfl_sync(g.mask, linked[0] ? 1u : 0u, at), l1 = __shfl_sync(g.mask, linked[1] ? 1u : 0u, at);
+        if (k / n == 0u ? l0 : l1) break;
+      }
     }
     *fp_io = fp;
     return passed;
   }
 
-  // Return k chained queue chunks starting at c to the base pool: lanes find
-  // their chunk as in walk_drained, clear its tag and page size (and its
-  // entries for chunk queues), and all of a round are published with one
-  // reservation on the reuse ring.  Returns the chunk after the last one.
-  // Collective over g.
+  // Return k chained queue chunks starting at c to the base pool: index
+  // i = u x n + r (two per lane and round) finds its chunk as in walk_drained,
+  // clears its tag and page size (and its entries for chunk queues), and all
+  // of a round are published with one reservation on the reuse ring.
+  // Returns the chunk after the last one.  Collective over g.
   __device__ static uint32_t recycle_run(HeapCore* h, ClassState* q, const Group& g, uint32_t c, uint32_t k) {
     const uint32_t n = static_cast<uint32_t>(g.size), r = static_cast<uint32_t>(g.rank);
+    const int prev_lane = lane_of_rank(g.mask, r == 0u ? static_cast<int>(n) - 1 : static_cast<int>(r) - 1);
     ReuseQueue* rq = &h->reuse[0];
     uint32_t range = ld_relaxed(&h->meta[c].vstart) / kQcSpots;
     for (uint32_t guard = 0; k > 0u && guard < (1u << 16); ++guard) {
-      const uint32_t want = k < n ? k : n;
-      uint32_t mine = kEmpty, nx = kEmpty;
-      if (r < want) {
-        mine = r == 0u ? c : recall_range(h, q, range + r);
-        if (mine != kEmpty) nx = ld_acquire(&h->meta[mine].next);
+      const uint32_t want = k < 2u * n ? k : 2u * n;
+      uint32_t mine[2] = {kEmpty, kEmpty}, nx[2] = {kEmpty, kEmpty};
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const uint32_t i = static_cast<uint32_t>(u) * n + r;
+        if (i < want) mine[u] = i == 0u ? c : recall_range(h, q, range + i);
       }
-      const uint32_t prev_nx = __shfl_sync(g.mask, nx, lane_of_rank(g.mask, r == 0u ? 0 : static_cast<int>(r) - 1));
-      const bool ok = r < want && (r == 0u || (mine != kEmpty && mine == prev_nx)) && nx < kInstalling;
-      const uint32_t bad = __ballot_sync(g.mask, !ok);
-      const uint32_t L = bad ? first_rank(g, bad) : n;
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+        if (mine[u] != kEmpty) nx[u] = ld_acquire(&h->meta[mine[u]].next);
+      bool ok[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const uint32_t i = static_cast<uint32_t>(u) * n + r;
+        const uint32_t same = __shfl_sync(g.mask, nx[u], prev_lane);
+        const uint32_t wrap = __shfl_sync(g.mask, nx[u > 0 ? u - 1 : 0], prev_lane);
+        const uint32_t prev = r > 0u ? same : wrap;
+        ok[u] = i < want && (i == 0u || (mine[u] != kEmpty && mine[u] == prev)) && nx[u] < kInstalling;
+      }
+      const uint32_t b0 = __ballot_sync(g.mask, !ok[0]), b1 = __ballot_sync(g.mask, !ok[1]);
+      const uint32_t L = b0 ? first_rank(g, b0) : (b1 ? n + first_rank(g, b1) : 2u * n);
       if (L == 0u) {   // a chunk behind front_ptr without a successor: the chain is broken
         if (g.is_leader()) set_status(h, kErrCorrupt);
         break;
       }
-      const uint32_t after = __shfl_sync(g.mask, nx, lane_of_rank(g.mask, static_cast<int>(L) - 1));
-      if (r < L) {
-        if (q->clean_on_recycle) clean_queue_chunk(h, mine);
-        st_relaxed(&h->meta[mine].size, 0u);
-        st_relaxed(&h->meta[mine].page_size, 0u);
-        __threadfence();
+      const int last = lane_of_rank(g.mask, static_cast<int>((L - 1u) % n));
+      const uint32_t a0 = __shfl_sync(g.mask, nx[0], last), a1 = __shfl_sync(g.mask, nx[1], last);
+      const uint32_t after = (L - 1u) / n == 0u ? a0 : a1;
+      bool any = false;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const uint32_t i = static_cast<uint32_t>(u) * n + r;
+        if (i < L) {
+          if (q->clean_on_recycle) clean_queue_chunk(h, mine[u]);
+          st_relaxed(&h->meta[mine[u]].size, 0u);
+          st_relaxed(&h->meta[mine[u]].page_size, 0u);
+          any = true;
+        }
       }
+      if (any) __threadfence();
       __syncwarp(g.mask);
       uint32_t pos = 0, take = L;
       if (g.is_leader()) {
@@ -671,9 +715,13 @@ struct VlStore {
       }
       pos = bcast(g, pos);
       take = bcast(g, take);
-      if (r < take) {
-        uint32_t* sl = rq->ring + ((pos + r) & (kReuseSize - 1u));
-        if (wait_slot_empty(h, sl)) st_release(sl, mine);
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const uint32_t i = static_cast<uint32_t>(u) * n + r;
+        if (i < take) {
+          uint32_t* sl = rq->ring + ((pos + i) & (kReuseSize - 1u));
+          if (wait_slot_empty(h, sl)) st_release(sl, mine[u]);
+        }
       }
       c = after;
       range += L;
