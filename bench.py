@@ -69,6 +69,7 @@ def parse_args():
     ap.add_argument("--no-churn", action="store_true", help="skip the churn measurement")
     ap.add_argument("--churn-rounds", type=int, default=1000)
     ap.add_argument("--serving-seconds", type=float, default=1.0)
+    ap.add_argument("--no-config1", action="store_true", help="skip the 65,536 x 64 B page-based configuration")
     return ap.parse_args()
 
 
@@ -231,7 +232,9 @@ def run_cells(arm, cells, n, block, stream, ptrs, counters, flush, steps, warmup
     `warmup` untimed repetitions, then `steps` timed ones, each a flushed,
     event-timed alloc launch, an untimed pattern write + verify, and a flushed,
     event-timed free launch.  Optionally one end-to-end repetition through the
-    C ABI with host buffers.  Returns {cell: (alloc_ms list, free_ms list, e2e_ms)}."""
+    C ABI with host buffers.  Returns {cell: (alloc_ms list, free_ms list, e2e_ms,
+    (cold alloc_ms, cold free_ms))}: the cold pair is repetition 0, the first
+    burst on the fresh heap (it is also the first warm-up repetition)."""
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     res = {}
     if e2e:
@@ -242,6 +245,7 @@ def run_cells(arm, cells, n, block, stream, ptrs, counters, flush, steps, warmup
         t0 = time.perf_counter()
         arm.open(v)
         a_ms, f_ms = [], []
+        cold = None
         for rep in range(warmup + steps):
             with torch.cuda.stream(stream):
                 flush.add_(1)
@@ -259,6 +263,7 @@ def run_cells(arm, cells, n, block, stream, ptrs, counters, flush, steps, warmup
                 a_ms.append(ev[0].elapsed_time(ev[1]))
                 f_ms.append(ev[2].elapsed_time(ev[3]))
             if rep == 0:
+                cold = (ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3]))
                 flags = arm.flags()
                 if flags & ~1:
                     why = arm.detail() if hasattr(arm, "detail") else ""
@@ -281,10 +286,75 @@ def run_cells(arm, cells, n, block, stream, ptrs, counters, flush, steps, warmup
         arm.close()
         if flags & ~1:
             raise BenchAbort(f"device error flags {flags} after {v}:{size} {why}")
-        res[(v, size)] = (a_ms, f_ms, e2e_ms)
+        res[(v, size)] = (a_ms, f_ms, e2e_ms, cold)
         print(f"[bench] {tag} {v}:{size} alloc {np.mean(a_ms):.4f} ms free {np.mean(f_ms):.4f} ms "
-              f"({time.perf_counter() - t0:.2f}s)", file=sys.stderr, flush=True)
+              f"cold alloc {cold[0]:.4f} ms free {cold[1]:.4f} ms ({time.perf_counter() - t0:.2f}s)",
+              file=sys.stderr, flush=True)
     return res
+
+
+def cold_summary(res, n) -> dict:
+    """The first burst on every fresh heap: repetition 0 of each cell, the case
+    where every request must create chunks."""
+    per, ops, ms = {}, 0.0, 0.0
+    for (v, s), (_, _, _, (ca, cf)) in res.items():
+        per[f"{v}:{s}"] = {"alloc_ms": round(ca, 4), "free_ms": round(cf, 4),
+                           "mops": round(2.0 * n / ((ca + cf) * 1e-3) / 1e6, 2)}
+        ops += 2.0 * n
+        ms += ca + cf
+    worst = max(per.items(), key=lambda kv: kv[1]["alloc_ms"])
+    return {"value": round(ops / (ms * 1e-3) / 1e6, 3), "unit": "Mops/s", "ms_total": round(ms, 3),
+            "worst_alloc": {"cell": worst[0], "alloc_ms": worst[1]["alloc_ms"]},
+            "what": "repetition 0 of every cell: one alloc launch of n threads on a fresh heap (every chunk is "
+                    "created in it) and the free launch after it, event-timed, L2 flushed before each",
+            "per_cell": per}
+
+
+def config1_bench(arm_cls, stream, steps=10) -> dict:
+    """The single-instantiation configuration: page-based standard queues, 1 GiB
+    heap, one launch of 65,536 threads (256 per block) each allocating 64 B;
+    after each alloc launch the payload is written and verified (untimed), then
+    one launch frees everything; 10 repetitions on one heap.  Reported the way
+    the reference's harness reports it (src/main.cu:146-167): the mean over all
+    repetitions, the first (cold) one included; the warm mean beside it."""
+    n, size, block = 1 << 16, 64, 256
+    arm = arm_cls(GiB)
+    ptrs = torch.zeros(n, dtype=torch.int64, device="cuda")
+    counters = torch.zeros(2, dtype=torch.int64, device="cuda")
+    flush = torch.zeros(64 << 20, dtype=torch.int32, device="cuda")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    a_ms, f_ms = [], []
+    with StdoutToStderr():
+        arm.open("P")
+        try:
+            for rep in range(steps):
+                with torch.cuda.stream(stream):
+                    flush.add_(1)
+                    ev[0].record(stream)
+                    arm.alloc(n, size, ptrs, block, stream)
+                    ev[1].record(stream)
+                    arm.write(ptrs, n, size, SEED + rep, stream)
+                    arm.verify(ptrs, n, size, SEED + rep, counters, stream)
+                    flush.add_(1)
+                    ev[2].record(stream)
+                    arm.free(n, ptrs, block, stream)
+                    ev[3].record(stream)
+                stream.synchronize()
+                a_ms.append(ev[0].elapsed_time(ev[1]))
+                f_ms.append(ev[2].elapsed_time(ev[3]))
+            flags = arm.flags()
+        finally:
+            arm.close()
+    nulls, bad = counters.tolist()
+    mean = float(np.mean(a_ms) + np.mean(f_ms))
+    warm = float(np.mean(a_ms[1:]) + np.mean(f_ms[1:]))
+    return {"workload": "P, 1 GiB heap, 65,536 threads x 64 B (256 per block), 10 repetitions on one heap",
+            "value": round(2.0 * n / (mean * 1e-3) / 1e6, 3), "unit": "Mops/s",
+            "what": "mean over all 10 repetitions, the first (cold) one included, as src/main.cu:146-167 averages",
+            "warm_mops": round(2.0 * n / (warm * 1e-3) / 1e6, 3),
+            "cold_ms": {"alloc": round(a_ms[0], 4), "free": round(f_ms[0], 4)},
+            "alloc_ms": [round(x, 4) for x in a_ms], "free_ms": [round(x, 4) for x in f_ms],
+            "null_results": nulls, "bad_words": bad, "flags": flags}
 
 
 def cpu_baseline(cells, n, heap_bytes) -> dict:
@@ -343,7 +413,7 @@ def roofline(res, n, steps) -> dict:
     distinct hot lines (2, or 1 for chunk free)."""
     import ouroboros_b200 as ob
     per = {}
-    for (v, size), (a, f, _) in res.items():
+    for (v, size), (a, f, _, _) in res.items():
         for kern, ms in (("alloc", a), ("free", f)):
             t = per.setdefault((v, kern), [0.0, 0])
             t[0] += float(np.sum(ms))
@@ -638,7 +708,7 @@ def main():
     per_cell = {}
     total_ms = alloc_ms = free_ms = 0.0
     e2e_ms = 0.0
-    for (v, s), (a, f, e) in res.items():
+    for (v, s), (a, f, e, _) in res.items():
         per_cell[f"{v}:{s}"] = {"alloc_ms": round(float(np.mean(a)), 5), "free_ms": round(float(np.mean(f)), 5),
                                 "mops": round(2.0 * n / ((np.mean(a) + np.mean(f)) * 1e-3) / 1e6, 2)}
         total_ms += float(np.sum(a) + np.sum(f))
@@ -655,7 +725,7 @@ def main():
         counters_x = torch.zeros(2, dtype=torch.int64, device="cuda")
         try:
             rx = run_cells(arm, extra_cells, n, args.block, stream, ptrs, counters_x, flush, 2, 1, tag="extra")
-            for (v, s), (a, f, _) in rx.items():
+            for (v, s), (a, f, _, _) in rx.items():
                 extra[f"{v}:{s}"] = {"alloc_ms": round(float(np.mean(a)), 5), "free_ms": round(float(np.mean(f)), 5)}
             extra["null_results_per_repetition"] = int(counters_x[0].item()) // 3
         except BenchAbort as exc:
@@ -678,7 +748,13 @@ def main():
         "timed_region": "per cell: W warm-up + K timed repetitions on a fresh heap; value = all mallocs and frees / "
                         "summed alloc + free kernel time",
         "clocks": clocks, "per_cell": per_cell,
+        "cold": cold_summary(res, n),
     }
+    if rank == 0 and not args.no_config1:
+        try:
+            out["config1"] = config1_bench(ReferenceArm if args.impl == "reference" else OursArm, stream)
+        except Exception as exc:   # reported, the headline stands
+            out["config1"] = {"error": str(exc)[:300]}
     if args.impl == "reference":
         out["impl"] = "reference"
         out["gpu_launches"] = 0

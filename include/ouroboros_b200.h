@@ -102,8 +102,8 @@ typedef struct {
   uint64_t timeouts;          /* bounded waits that gave up                 */
   uint64_t chunk_allocs;      /* chunk allocations (Statistics.h:11)        */
   uint64_t next_free_chunk;   /* Memory::next_free_chunk                    */
-  uint32_t timeout_sites;     /* one bit per kind of wait that gave up: 1 semaphore rounds,
-                                 2 semaphore CAS, 4 semaphore reservation, 8 queue slot still
+  uint32_t timeout_sites;     /* one bit per kind of wait that gave up: 1, 2 unused, 4 a group
+                                 in deficit waiting for its pages, 8 queue slot still
                                  full, 16 queue slot never written, 32 array index entry,
                                  64 linked successor, 128 walk length, 256 walks meeting
                                  recycled chunks, 512 / 1024 chunk reuse ring read / write,
@@ -147,8 +147,10 @@ int ouro_check_allocations(ouro_heap* h, void* const* d_ptrs, uint32_t n, uint32
  * exit).  It covers heaps of up to 1 GiB of chunk data (max_chunks <= 131072);
  * larger heaps return OURO_ERR_TOO_LARGE.  The current device must be the
  * heap's.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) and keeps it; make that first call before any stream
- * capture.  Each call clears the bitmap words its heap uses and *d_report
+ * (cudaGetSymbolAddress) and keeps it with the device's current context; make
+ * that first call before any stream capture.  A call in a new context (after
+ * cudaDeviceReset) looks the address up again.  Each call clears the bitmap
+ * words its heap uses and *d_report
  * (an ouro_alloc_report in DEVICE memory, filled in stream order; nothing is
  * synchronized).  All calls share the one array: calls whose work overlaps on
  * the GPU (other streams, or other host threads without ordering) race and

@@ -21,8 +21,9 @@ LIB = os.path.join(LIB_DIR, "libouroboros_b200.so")
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
+OBJ_DIR = os.path.join(HERE, "_build")
 
 
 def nvcc() -> str:
@@ -49,15 +50,30 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Each translation unit is compiled on its own, all at once, then linked."""
     if not force and up_to_date():
         return LIB
     os.makedirs(LIB_DIR, exist_ok=True)
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", LIB + ".tmp", *sources()]
-    if verbose:
-        print(" ".join(cmd), flush=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    procs = []
+    for src in sources():
+        obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
+        cmd = [nvcc(), *NVCC_FLAGS, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    errors = []
+    for obj, p in procs:
+        _, err = p.communicate()
+        if p.returncode != 0:
+            errors.append(f"{obj}:\n{err[-4000:]}")
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
+    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB + ".tmp",
+           *[obj for obj, _ in procs]]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed:\n{res.stderr[-4000:]}")
+        raise RuntimeError(f"nvcc link failed:\n{res.stderr[-4000:]}")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

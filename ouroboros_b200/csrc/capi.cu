@@ -234,7 +234,10 @@ __global__ void k_peak_hot(uint32_t* a, unsigned long long* a64, int iters, int 
   if (acc == 0x9E3779B9u) *sink = acc;
 }
 
-bool g_heap_limit_set = false;
+// Devices whose CUDA device-heap limit was raised (the limit is per device).
+constexpr int kMaxDevices = 64;
+bool g_heap_limit_set[kMaxDevices] = {};
+std::mutex g_heap_limit_mu;
 
 }  // namespace
 
@@ -258,22 +261,28 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
   *out = nullptr;
   Layout L;
   if (!compute_layout(variant / 2, heap_bytes, &L)) return OURO_ERR_ARG;
-  if (!g_heap_limit_set) {
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return OURO_ERR_CUDA;
+  {
     // the reference reserves 500 MiB of CUDA device heap for requests > 32 KiB
-    // (Parameters.h:49, MemoryInitialization.cuh:130-134); only possible
-    // before the first kernel that calls device malloc
-    size_t cur = 0;
-    cudaDeviceGetLimit(&cur, cudaLimitMallocHeapSize);
-    if (cur < (500ull << 20)) cudaDeviceSetLimit(cudaLimitMallocHeapSize, 500ull << 20);
-    (void)cudaGetLastError();
-    g_heap_limit_set = true;
+    // (Parameters.h:49, MemoryInitialization.cuh:130-134); a per-device
+    // limit, only settable before that device's first kernel that calls
+    // device malloc
+    std::lock_guard<std::mutex> lock(g_heap_limit_mu);
+    if (device >= 0 && device < kMaxDevices && !g_heap_limit_set[device]) {
+      size_t cur = 0;
+      cudaDeviceGetLimit(&cur, cudaLimitMallocHeapSize);
+      if (cur < (500ull << 20)) cudaDeviceSetLimit(cudaLimitMallocHeapSize, 500ull << 20);
+      (void)cudaGetLastError();
+      g_heap_limit_set[device] = true;
+    }
   }
   ouro_heap* h = new (std::nothrow) ouro_heap();
   if (!h) return OURO_ERR_NOMEM;
   h->variant = variant;
   h->heap_bytes = heap_bytes;
   h->L = L;
-  cudaGetDevice(&h->device);
+  h->device = device;
   if (cudaMalloc(&h->raw, L.alloc_bytes) != cudaSuccess) {
     (void)cudaGetLastError();
     delete h;
@@ -327,7 +336,7 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
       q.ring_mask = kVqSize - 1u;
       q.page_cap = kVqSize * kQcSpots;
     } else {
-      q.page_cap = static_cast<uint32_t>(SemWord::kMaxCount);
+      q.page_cap = 1u << 30;   // linked queues are unbounded; positions are 32-bit
       q.skip = reinterpret_cast<uint32_t*>(h->base + L.skip_off) + static_cast<size_t>(c) * kSkipSlots;
     }
   }
@@ -447,8 +456,8 @@ int ouro_state(ouro_heap* h, uint64_t* out) {
     const ClassState& q = core.cls[c];
     uint64_t* o = out + 7 + 12 * c;
     o[0] = static_cast<uint64_t>(SemWord::count(q.sem.v));
-    o[1] = static_cast<uint64_t>(SemWord::exp_chunks(q.sem.v)) * q.ppc;
-    o[2] = SemWord::reserved(q.sem.v);
+    o[1] = 0;   // expected and reserved pages of the reference's semaphore: none at quiescence
+    o[2] = SemWord::is_short(q.sem.v) ? 1u : 0u;
     o[3] = q.front.v;
     o[4] = q.back.v;
     o[5] = chunk_based && kind != 2 ? static_cast<uint64_t>(static_cast<int64_t>(q.entries.v)) : 0u;
@@ -559,8 +568,8 @@ int ouro_check_heap(ouro_heap* h, ouro_heap_report* out) {
     out->owned_pages[c] = hr[c];
     out->free_pages_meta[c] = chunk_based ? hr[12 + c] : static_cast<uint64_t>(q.back.v - q.front.v);
     out->sem_count[c] = SemWord::count(q.sem.v);
-    out->sem_expected[c] = static_cast<uint64_t>(SemWord::exp_chunks(q.sem.v)) * q.ppc;
-    out->sem_reserved[c] = SemWord::reserved(q.sem.v);
+    out->sem_expected[c] = 0;   // no expected pages: groups in deficit own the chunks they add
+    out->sem_reserved[c] = SemWord::is_short(q.sem.v) ? 1u : 0u;   // an addition fell short, unresolved
   }
   out->data_chunks = hr[24];
   out->bad = hr[25];
@@ -577,26 +586,27 @@ int ouro_prefill(ouro_heap* h, uint64_t size, uint64_t pages, uint64_t* out_page
   if (chunks >= h->L.max_chunks) return OURO_ERR_ARG;
   if (out_pages) *out_pages = 0;
   if (chunks == 0) return OURO_OK;
-  uint32_t* d = nullptr;
-  if (cudaMalloc(&d, 16) != cudaSuccess) return OURO_ERR_NOMEM;
+  // the work counter and the result live in the heap's control block: no
+  // allocation, so no device-wide synchronization
+  uint32_t* d_next = &h->dev->prefill_next.v;
+  unsigned long long* d_done = &h->dev->prefill_done.v;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  cudaError_t e = cudaMemsetAsync(d, 0, 16, s);
+  cudaError_t e = cudaMemsetAsync(d_next, 0, sizeof(uint32_t), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_done, 0, sizeof(unsigned long long), s);
   if (e == cudaSuccess) {
     dispatch(h->variant, [&](auto v) {
       constexpr int V = decltype(v)::value;
       const unsigned warps = static_cast<unsigned>((chunks + 31u) / 32u);
       const unsigned blocks = warps < 148u * 8u ? (warps + 7u) / 8u : 148u;
       k_prefill<V><<<blocks, 256, 0, s>>>(reinterpret_cast<Ouroboros<V>*>(h->dev), static_cast<uint32_t>(cls),
-                                          static_cast<uint32_t>(chunks), d,
-                                          reinterpret_cast<unsigned long long*>(d + 2));
+                                          static_cast<uint32_t>(chunks), d_next, d_done);
       return 0;
     });
     e = cudaGetLastError();
   }
   unsigned long long done = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&done, d + 2, sizeof(done), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&done, d_done, sizeof(done), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  cudaFree(d);
   if (out_pages) *out_pages = done * ppc;
   return cuda_rc(e);
 }
@@ -642,8 +652,9 @@ int ouro_scan_stats(ouro_heap* h, uint64_t* out, int clear) {
 
 int ouro_measure_atomics(int mode, double* gops) {
   if (!gops || mode < 0 || mode > 2) return OURO_ERR_ARG;
-  int sms = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  int sms = 0, dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return OURO_ERR_CUDA;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const uint32_t N = 1u << 22;   // 16 MiB: L2 resident
   uint32_t* a = nullptr;
   if (cudaMalloc(&a, N * 4u + 256u) != cudaSuccess) return OURO_ERR_NOMEM;
@@ -694,24 +705,58 @@ namespace {
 
 // Device address of ouro_noalloc_bitmap on each device.  On the host the
 // array's name is only a stand-in for the device object, so the address is
-// asked from the runtime once per device, with that device current.
+// asked from the runtime once per device, with that device current, and kept
+// together with the context it belongs to: after a cudaDeviceReset the
+// device's next context loads the library's module again, at an address the
+// old one says nothing about, so a changed context means a fresh look-up.
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
-uint32_t* g_noalloc_addr[kNoAllocMaxDevices] = {};
+struct NoAllocSlot {
+  void* ctx;
+  uint32_t* addr;
+};
+NoAllocSlot g_noalloc[kNoAllocMaxDevices] = {};
+
+// The driver's cuCtxGetCurrent, reached through the runtime so that the
+// library does not link the driver library itself.
+using CtxGetCurrent = int (*)(void**);
+CtxGetCurrent ctx_get_current() {
+  static CtxGetCurrent fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult st;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &st) != cudaSuccess ||
+        st != cudaDriverEntryPointSuccess) {
+      (void)cudaGetLastError();
+      p = nullptr;
+    }
+    return reinterpret_cast<CtxGetCurrent>(p);
+  }();
+  return fn;
+}
+
+void* current_context() {
+  void* ctx = nullptr;
+  const CtxGetCurrent fn = ctx_get_current();
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
 
 int noalloc_bitmap(int device, uint32_t** out) {
   if (device < 0 || device >= kNoAllocMaxDevices) return OURO_ERR_ARG;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
+  NoAllocSlot& slot = g_noalloc[device];
+  void* ctx = current_context();
+  if (!slot.addr || !ctx || slot.ctx != ctx) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, ouro_noalloc_bitmap);
     if (e != cudaSuccess || !p) {
       (void)cudaGetLastError();
       return OURO_ERR_CUDA;
     }
-    g_noalloc_addr[device] = static_cast<uint32_t*>(p);
+    slot.addr = static_cast<uint32_t*>(p);
+    slot.ctx = ctx ? ctx : current_context();   // the look-up made the context current
   }
-  *out = g_noalloc_addr[device];
+  *out = slot.addr;
   return OURO_OK;
 }
 

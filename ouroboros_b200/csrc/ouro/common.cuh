@@ -60,15 +60,16 @@ __host__ __device__ constexpr uint32_t class_page_shift(uint32_t cls) { return c
 __host__ __device__ constexpr uint32_t instance_factor(uint32_t inst) { return inst == 0u ? 1u : 4u; }
 __host__ __device__ constexpr uint32_t instance_mask_words(uint32_t inst) { return inst == 0u ? 16u : 1u; }
 
-// Helper.cuh:11-18 + 42-45: the queue index of a request size, restated.
+// Helper.cuh:11-18 + 42-45: the queue index of a request size, restated, on
+// the full 64-bit size (a request above 4 GiB must not wrap to a small power
+// of two).  n = 0 gives -1.
 __host__ __device__ inline int next_pow2_pow(uint64_t n) {
-  uint32_t v = static_cast<uint32_t>(n);
 #ifdef __CUDA_ARCH__
-  int lz = __clz(static_cast<int>(v));
+  int lz = __clzll(static_cast<long long>(n));
 #else
-  int lz = v ? __builtin_clz(v) : 32;
+  int lz = n ? __builtin_clzll(n) : 64;
 #endif
-  return ((n & (n - 1u)) == 0u) ? 32 - lz - 1 : 32 - lz;
+  return ((n & (n - 1u)) == 0u) ? 64 - lz - 1 : 64 - lz;
 }
 
 // Size -> class id (0..11), or -1 for sizes served by the CUDA device heap.

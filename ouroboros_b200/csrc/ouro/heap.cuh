@@ -86,6 +86,10 @@ struct alignas(128) HeapCore {
   // diagnostic counters, only written when built with OURO_SCAN_STATS (their
   // meaning per heap kind is listed at ouro_scan_stats in the C header)
   Line<unsigned long long> scan[kScanCounters];
+  // work counter and result of the host's bulk pre-population call, kept in
+  // the heap so that the call allocates nothing
+  Line<uint32_t> prefill_next;
+  Line<unsigned long long> prefill_done;
 };
 
 constexpr size_t kCoreBytes = 16384;
@@ -94,9 +98,9 @@ static_assert(sizeof(HeapCore) <= kCoreBytes, "control block grew past its regio
 __device__ __forceinline__ void set_status(HeapCore* h, uint32_t bits) { atomicOr(&h->status.v, bits); }
 // Bounded waits, one bit each in HeapCore::timeout_sites when they give up.
 enum WaitSite : uint32_t {
-  kWaitSemRounds = 1u << 0,    // semaphore: rounds of a group's acquisition
-  kWaitSemCas = 1u << 1,       // semaphore: CAS retries
-  kWaitSemReserve = 1u << 2,   // semaphore: reserved pages that do not arrive
+  kWaitSemRounds = 1u << 0,    // (unused: the semaphore has no acquisition rounds)
+  kWaitSemCas = 1u << 1,       // (unused: the semaphore has no CAS loop on its hot path)
+  kWaitSemReserve = 1u << 2,   // semaphore: pages of a group in deficit that do not arrive
   kWaitSlotEmpty = 1u << 3,    // queue slot still holding the previous lap's entry
   kWaitSlotFull = 1u << 4,     // queue slot whose producer does not write it
   kWaitIndexEntry = 1u << 5,   // virtualized array: queue chunk of a range
@@ -163,6 +167,7 @@ __host__ inline bool compute_layout(int kind, unsigned long long heap_bytes, Lay
 // The chunk reuse ring (queues/Queue_impl.cuh:20-66): FIFO of whole chunks
 // that left a queue.  take() serves up to k chunks for one group.
 __device__ inline uint32_t reuse_take(HeapCore* h, ReuseQueue* r, uint32_t k, uint32_t* first_pos) {
+  if (ld_relaxed(&r->count.v) <= 0) return 0u;   // empty: no atomics (a cold heap grows by the bump pointer)
   int32_t old = atomicSub(&r->count.v, static_cast<int32_t>(k));
   uint32_t got = old <= 0 ? 0u : (static_cast<uint32_t>(old) < k ? static_cast<uint32_t>(old) : k);
   if (got < k) atomicAdd(&r->count.v, static_cast<int32_t>(k - got));
@@ -218,8 +223,17 @@ __device__ inline uint32_t alloc_chunk_rounds(HeapCore* h, const Group& g, uint3
   unsigned long long first = 0;
   if (g.is_leader()) {
     from_reuse = reuse_take(h, r, k, &rpos);
-    if (from_reuse < k) first = atomicAdd(&h->next_free_chunk.v, (unsigned long long)(k - from_reuse) * factor);
-    atomicAdd(&h->chunk_allocs.v, (unsigned long long)k);
+    bool bumped = false;
+    if (from_reuse < k) {
+      // past the end the bump pointer is not moved again: an exhausted heap
+      // answers with loads only
+      first = ld_relaxed(&h->next_free_chunk.v);
+      if (first + factor < h->max_chunks) {
+        first = atomicAdd(&h->next_free_chunk.v, (unsigned long long)(k - from_reuse) * factor);
+        bumped = true;
+      }
+    }
+    if (from_reuse || bumped) atomicAdd(&h->chunk_allocs.v, (unsigned long long)k);
   }
   from_reuse = bcast(g, from_reuse);
   rpos = bcast(g, rpos);

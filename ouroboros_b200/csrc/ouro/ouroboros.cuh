@@ -32,8 +32,10 @@ struct Ouroboros : HeapCore {
     const Group g = group_by(active, static_cast<uint64_t>(cls + 1));
     if (cls < 0) {
       // Ouroboros<>::malloc: next power of two from the CUDA device heap
-      int p2 = next_pow2_pow(size);
-      return ::malloc(static_cast<size_t>(1) << (p2 < 0 ? 0 : p2));
+      // (a size whose power of two does not fit in size_t cannot be served)
+      const int p2 = next_pow2_pow(size);
+      if (p2 >= 63) return nullptr;
+      return ::malloc(static_cast<size_t>(1) << p2);
     }
     ClassState* q = &this->cls[cls];
     if constexpr (kPageBased) return page_alloc<Store>(this, q, g);
@@ -43,15 +45,14 @@ struct Ouroboros : HeapCore {
   // Bulk pre-population (the reference's preFillQueue / enqueueInitialChunk,
   // PageQueue.cuh:42-49, PageQueue_impl.cuh:40-53, ChunkQueue_impl.cuh:69-77):
   // the group adds k fresh chunks to class cls and publishes all their pages
-  // as free, through the same path an elected allocation takes (the semaphore
-  // is told to expect k chunks first).  Collective over the calling lanes of
-  // one warp, k <= their number.  Returns the chunks added.
+  // as free, through the path a group in deficit takes to add chunks.
+  // Collective over the calling lanes of one warp, k <= their number.
+  // Returns the chunks added.
   __device__ __forceinline__ uint32_t prefill(uint32_t cls, uint32_t k) {
     const Group g = make_group(__activemask());
     ClassState* q = &this->cls[cls];
-    if (g.is_leader()) atomicAdd(&q->sem.v, static_cast<unsigned long long>(k) << SemWord::kExpShift);
-    if constexpr (kPageBased) return page_grow<Store>(this, q, g, k);
-    else return chunk_grow<Store>(this, q, g, k);
+    if constexpr (kPageBased) return page_grow<Store>(this, q, g, k, false);
+    else return chunk_grow<Store>(this, q, g, k, false);
   }
 
   __device__ __forceinline__ void free(void* ptr) {

@@ -68,6 +68,7 @@ __device__ __forceinline__ uint32_t reserve_class_pages(HeapCore* h, ClassState*
 __device__ __forceinline__ uint32_t queue_chunks_for(uint32_t entries) { return (entries + kQcSpots - 1u) / kQcSpots; }
 
 __device__ inline uint32_t commit_budget(HeapCore* h, uint32_t k, uint32_t factor, uint32_t e0, uint32_t per) {
+  if (ld_relaxed(&h->budget.v) + factor > h->budget_limit) return 0u;   // spent: no atomics
   for (uint32_t kk = k; kk; kk >>= 1) {
     const unsigned long long d = static_cast<unsigned long long>(kk) * factor + queue_chunks_for(e0 + kk * per) -
                                  queue_chunks_for(e0);
@@ -80,11 +81,13 @@ __device__ inline uint32_t commit_budget(HeapCore* h, uint32_t k, uint32_t facto
 
 // ============================================================ page queues
 
-// The semaphore elected this group to add k chunks (the wait lambda of
+// The group adds k chunks to its class (the wait lambda of
 // PageQueue_impl.cuh:114-125): allocate, describe, publish all their pages at
-// the back with one position reservation, and credit the semaphore.
+// the back with one position reservation, and credit the semaphore.  `owed`:
+// the chunks cover a deficit (semaphore demand), so getting fewer marks the
+// class short; pre-population owes nothing.
 template <class Store>
-__device__ uint32_t page_grow(HeapCore* h, ClassState* q, const Group& g, uint32_t k) {
+__device__ uint32_t page_grow(HeapCore* h, ClassState* q, const Group& g, uint32_t k, bool owed) {
   const uint32_t factor = instance_factor(q->inst);
   uint32_t kk = 0;   // chunks this group may add
   if (g.is_leader()) {
@@ -117,7 +120,10 @@ __device__ uint32_t page_grow(HeapCore* h, ClassState* q, const Group& g, uint32
     __syncwarp(g.mask);
     __threadfence();
   }
-  if (g.is_leader()) sem_fulfil(q, E, k);
+  if (g.is_leader()) {
+    if (owed && got < k) sem_mark_short(q);
+    sem_signal(q, E);
+  }
   return got;
 }
 
@@ -126,7 +132,7 @@ __device__ void* page_alloc(HeapCore* h, ClassState* q, const Group& g) {
 #ifdef OURO_SCAN_STATS
   const long long t0 = clock64();
 #endif
-  uint32_t granted = sem_acquire(h, q, g, [&](uint32_t k) { return page_grow<Store>(h, q, g, k); });
+  uint32_t granted = sem_acquire(h, q, g, [&](uint32_t k) { page_grow<Store>(h, q, g, k, true); });
 #ifdef OURO_SCAN_STATS
   const long long t1 = clock64();
 #endif
@@ -323,9 +329,9 @@ __device__ void claim_pages(HeapCore* h, const Group& s, uint32_t c, uint32_t go
 }
 
 // The wait lambda of ChunkQueue_impl.cuh:86-100: k empty chunks, each with one
-// queue entry, then credit the semaphore.
+// queue entry, then credit the semaphore (`owed` as for page_grow).
 template <class Store>
-__device__ uint32_t chunk_grow(HeapCore* h, ClassState* q, const Group& g, uint32_t k) {
+__device__ uint32_t chunk_grow(HeapCore* h, ClassState* q, const Group& g, uint32_t k, bool owed) {
   const uint32_t factor = instance_factor(q->inst);
   uint32_t kk = k;
   if constexpr (Store::kKind != 0) {
@@ -359,7 +365,10 @@ __device__ uint32_t chunk_grow(HeapCore* h, ClassState* q, const Group& g, uint3
   if (mine) chunk_enqueue_group<Store>(h, q, make_group(em), c);
   __syncwarp(g.mask);
   __threadfence();
-  if (g.is_leader()) sem_fulfil(q, got * q->ppc, k);
+  if (g.is_leader()) {
+    if (owed && got < k) sem_mark_short(q);
+    sem_signal(q, got * q->ppc);
+  }
   return got;
 }
 
@@ -492,7 +501,7 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
 #ifdef OURO_SCAN_STATS
   long long t_begin = clock64(), t_claim = 0, t_deq = 0;
 #endif
-  uint32_t granted = sem_acquire(h, q, g, [&](uint32_t k) { return chunk_grow<Store>(h, q, g, k); });
+  uint32_t granted = sem_acquire(h, q, g, [&](uint32_t k) { chunk_grow<Store>(h, q, g, k, true); });
 #ifdef OURO_SCAN_STATS
   const long long t_sem = clock64() - t_begin;
 #endif

@@ -1,14 +1,34 @@
 // semaphore.cuh -- the per-class page semaphore.
 //
-// Same protocol as the reference's BulkSemaphore (BulkSemaphore_impl.cuh:
-// 116-232): a packed word of (count, expected, reserved); a fast path that
-// subtracts the group's demand, and a CAS path that either claims, reserves
-// and waits, or elects the group to allocate chunks.  Differences: the fields
-// are repacked (count 26 bits biased by 2^25, expected counted in whole chunks
-// with 19 bits, reserved 19 bits) so that neither expected nor reserved can
-// overflow at B200 thread counts; a group may allocate several chunks in one
-// election; every wait is bounded; allocation failure ends in a partial grant
-// instead of undefined behaviour.
+// It plays the role of the reference's BulkSemaphore (BulkSemaphore_impl.cuh:
+// 116-232): it counts a class's free pages, hands them to requesting groups
+// and decides when chunks are added.  Its protocol is this build's own: a
+// group never loops on a CAS of the hot word.
+//
+//   word = count (bits 0..37, biased by 2^37) | short (bit 38) | supply
+//          (bits 39..63, pages ever added, mod 2^25; topmost, so that its
+//          carry leaves the word)
+//
+// * A group of n lanes takes n pages with ONE fetch-add of -n.  If the count
+//   before it was >= n the pages are there: done (the warm path).
+// * Otherwise the group keeps its demand: the count goes below zero and the
+//   group owns the slice [max(-c0, 0), n - c0) of the class's deficit.  Every
+//   multiple of pages-per-chunk inside its slice is a chunk that this group
+//   adds itself.  Chunks being added always cover the deficit from 0 up to a
+//   multiple of pages-per-chunk, so the chunks a burst needs are created once
+//   each, in parallel, by the groups whose demand crossed them.  A lone thread
+//   therefore adds a chunk exactly when the count is 0, which is the
+//   reference's decision, so sequential replays stay bit-exact with it.
+// * Adding pages (new chunks, frees, pre-fill) adds to count and supply in one
+//   fetch-add.  The pages of a group that went into deficit exist once supply
+//   has advanced by its slice end since its fetch-add; it waits for that
+//   (bounded) before it takes queue entries.
+// * Out of chunks: a failed addition sets `short` and adds only the pages it
+//   got.  Groups that still wait then see `short`, hand their demand back and
+//   take what is there with fetch-adds (take_upto), retrying while pages
+//   remain, so exactly the available pages are served and the rest get
+//   nullptr.  `short` is cleared once the count is back at or above zero.
+// * Every wait is bounded and reports a timeout instead of hanging.
 #pragma once
 
 #include "heap.cuh"
@@ -16,156 +36,141 @@
 namespace ouro {
 
 struct SemWord {
-  static constexpr unsigned long long kCntMask = (1ull << 26) - 1u;
-  static constexpr unsigned long long kBias = 1ull << 25;
-  static constexpr uint32_t kExpShift = 26u;
-  static constexpr uint32_t kResShift = 45u;
-  static constexpr unsigned long long kFieldMask = (1ull << 19) - 1u;
+  static constexpr uint32_t kCntBits = 38u;
+  static constexpr unsigned long long kCntMask = (1ull << kCntBits) - 1u;
+  static constexpr unsigned long long kBias = 1ull << (kCntBits - 1u);
+  static constexpr unsigned long long kShort = 1ull << kCntBits;
+  static constexpr uint32_t kSupShift = kCntBits + 1u;
+  static constexpr uint32_t kSupBits = 64u - kSupShift;
+  static constexpr unsigned long long kSupMask = (1ull << kSupBits) - 1u;
   static constexpr unsigned long long kInit = kBias;
-  static constexpr long long kMaxCount = (1ll << 25) - 1;
 
   __host__ __device__ static long long count(unsigned long long v) {
     return static_cast<long long>(v & kCntMask) - static_cast<long long>(kBias);
   }
-  __host__ __device__ static uint32_t exp_chunks(unsigned long long v) {
-    return static_cast<uint32_t>((v >> kExpShift) & kFieldMask);
+  __host__ __device__ static uint32_t supply(unsigned long long v) {
+    return static_cast<uint32_t>((v >> kSupShift) & kSupMask);
   }
-  __host__ __device__ static uint32_t reserved(unsigned long long v) {
-    return static_cast<uint32_t>((v >> kResShift) & kFieldMask);
+  __host__ __device__ static bool is_short(unsigned long long v) { return (v & kShort) != 0u; }
+  // pages the supply field advanced from a to b (modular)
+  __host__ __device__ static uint32_t supply_since(unsigned long long a, unsigned long long b) {
+    return (supply(b) - supply(a)) & static_cast<uint32_t>(kSupMask);
   }
-  __host__ __device__ static unsigned long long make(long long c, uint32_t e, uint32_t r) {
-    return static_cast<unsigned long long>(c + static_cast<long long>(kBias)) |
-           (static_cast<unsigned long long>(e) << kExpShift) | (static_cast<unsigned long long>(r) << kResShift);
+  // fetch-add operands: count -= n; count += n (a hand-back, not supply);
+  // count += n and supply += n
+  __host__ __device__ static unsigned long long take(uint32_t n) { return 0ull - static_cast<unsigned long long>(n); }
+  __host__ __device__ static unsigned long long give(uint32_t n) { return static_cast<unsigned long long>(n); }
+  __host__ __device__ static unsigned long long add(uint32_t n) {
+    return static_cast<unsigned long long>(n) + (static_cast<unsigned long long>(n) << kSupShift);
   }
-  __host__ __device__ static unsigned long long sub(uint32_t n) { return ~static_cast<unsigned long long>(n) + 1ull; }
 };
 
-// count += pages (a free, or pages that arrived)
+// `short` is cleared once nothing is owed.  Every operation that sees the
+// flag with the count (after the operation) at or above zero retries the
+// clear a few times; `now` is the word as that operation left it.
+__device__ __forceinline__ void sem_maybe_clear_short(ClassState* q, unsigned long long now) {
+  for (uint32_t tries = 0; tries < 8u && SemWord::is_short(now) && SemWord::count(now) >= 0; ++tries) {
+    const unsigned long long seen = atomicCAS(&q->sem.v, now, now & ~SemWord::kShort);
+    if (seen == now) return;
+    now = seen;
+  }
+}
+
+// Pages arrived (new chunks, a free, pre-fill): count += pages, supply += pages.
 __device__ __forceinline__ void sem_signal(ClassState* q, uint32_t pages) {
-  if (pages) atomicAdd(&q->sem.v, static_cast<unsigned long long>(pages));
+  if (!pages) return;
+  const unsigned long long old = atomicAdd(&q->sem.v, SemWord::add(pages));
+  if (SemWord::is_short(old)) sem_maybe_clear_short(q, old + SemWord::add(pages));
 }
 
-// Chunks promised earlier arrived: count += got_pages, expected -= promised.
-__device__ __forceinline__ void sem_fulfil(ClassState* q, uint32_t got_pages, uint32_t promised_chunks) {
-  unsigned long long d = static_cast<unsigned long long>(got_pages) -
-                         (static_cast<unsigned long long>(promised_chunks) << SemWord::kExpShift);
-  atomicAdd(&q->sem.v, d);
-}
+// An addition of chunks fell short of what the class owes: waiting groups
+// resolve their demand against the pages that are there.
+__device__ __forceinline__ void sem_mark_short(ClassState* q) { atomicOr(&q->sem.v, SemWord::kShort); }
 
-// BulkSemaphore_impl.cuh:7-17 tryReduce
+// BulkSemaphore_impl.cuh:7-17 tryReduce: take n pages only if all of them are
+// there.  Used by the standard chunk queue to hand a fully free chunk back to
+// the pool; a CAS so that the count never dips for other groups (rare path).
 __device__ __forceinline__ bool sem_try_reduce(ClassState* q, uint32_t n) {
   if (n == 0) return true;
-  unsigned long long old = atomicAdd(&q->sem.v, SemWord::sub(n));
-  if (SemWord::count(old) - static_cast<long long>(n) < 0) {
-    atomicAdd(&q->sem.v, static_cast<unsigned long long>(n));
-    return false;
+  unsigned long long v = ld_relaxed(&q->sem.v);
+  for (uint32_t tries = 0; tries < 64u; ++tries) {
+    if (SemWord::count(v) < static_cast<long long>(n)) return false;
+    const unsigned long long seen = atomicCAS(&q->sem.v, v, v + SemWord::take(n));
+    if (seen == v) return true;
+    v = seen;
   }
-  return true;
+  return false;
+}
+
+// Take up to n pages that are there with fetch-adds only.  A group that took
+// more than was there hands the excess back; if the count is positive after
+// its hand-back (other groups' excess was in flight) and it still needs
+// pages, it tries again.  Returns the pages taken.
+__device__ inline uint32_t sem_take_upto(HeapCore* h, ClassState* q, uint32_t n) {
+  uint32_t got = 0;
+  for (uint32_t round = 0; got < n && round < 256u; ++round) {
+    const uint32_t want = n - got;
+    const unsigned long long old = atomicAdd(&q->sem.v, SemWord::take(want));
+    const long long c0 = SemWord::count(old);
+    const uint32_t t = c0 <= 0 ? 0u : (c0 < static_cast<long long>(want) ? static_cast<uint32_t>(c0) : want);
+    got += t;
+    if (t == want) break;
+    const unsigned long long now = atomicAdd(&q->sem.v, SemWord::give(want - t)) + SemWord::give(want - t);
+    sem_maybe_clear_short(q, now);
+    if (SemWord::count(now) <= 0) break;
+  }
+  return got;
 }
 
 // Acquire g.size pages of class q for the group.  Collective over the group;
 // the leader issues the atomics.  `grow(k)` is called collectively when the
-// group is elected to add k chunks; it must publish the new pages and call
-// sem_fulfil(q, pages, k), and return the number of chunks obtained.
-// Returns the number of pages granted (g.size, or fewer after an allocation
-// failure, 0 after a timeout).
+// group has to add k chunks; it publishes the pages it got, adds them with
+// sem_signal, and calls sem_mark_short if it got fewer than k chunks.
+// Returns the pages granted: g.size, or fewer when chunks ran out.
 template <typename Grow>
 __device__ inline uint32_t sem_acquire(HeapCore* h, ClassState* q, const Group& g, Grow&& grow) {
-  enum : uint32_t { kTake = 0, kAlloc = 1, kReserve = 2, kFail = 3 };
   const uint32_t n = static_cast<uint32_t>(g.size);
   const uint32_t ppc = q->ppc;
-  bool first = true;
-  bool failed_alloc = false;
-  for (uint32_t round = 0;; ++round) {
-    uint32_t mode = kFail, arg = 0;
-    if (g.is_leader()) {
-      if (round > kSpinLimit) {
-        note_timeout(h, kWaitSemRounds);
-        mode = kFail;
-      } else {
-        // fast path: one subtract (optimistic on the first round)
-        bool try_fast = first || SemWord::count(ld_relaxed(&q->sem.v)) >= static_cast<long long>(n);
-        first = false;
-        unsigned long long v;
-        bool done = false;
-        if (try_fast && !failed_alloc) {
-          v = atomicAdd(&q->sem.v, SemWord::sub(n));
-          if (SemWord::count(v) >= static_cast<long long>(n)) {
-            mode = kTake;
-            arg = n;
-            done = true;
-          } else {
-            atomicAdd(&q->sem.v, static_cast<unsigned long long>(n));
-          }
-        }
-        if (!done) {
-          v = ld_relaxed(&q->sem.v);
-          for (uint32_t tries = 0;; ++tries) {
-            long long c = SemWord::count(v);
-            uint32_t e = SemWord::exp_chunks(v);
-            uint32_t r = SemWord::reserved(v);
-            long long avail = c + static_cast<long long>(e) * ppc - r;
-            unsigned long long nv;
-            if (failed_alloc) {
-              // out of chunks: take whatever is there, once
-              uint32_t m = c <= 0 ? 0u : (c < n ? static_cast<uint32_t>(c) : n);
-              nv = SemWord::make(c - m, e, r);
-              mode = kTake;
-              arg = m;
-            } else if (avail < static_cast<long long>(n)) {
-              // Size the growth on the count without the transient dips of
-              // other groups' fast-path attempts (they add their pages back),
-              // so that a burst does not allocate chunks for phantom demand.
-              const long long settled = (c < 0 ? 0 : c) + static_cast<long long>(e) * ppc - r;
-              const long long deficit = static_cast<long long>(n) - settled;
-              uint32_t k = deficit <= 0 ? 1u : static_cast<uint32_t>((deficit + ppc - 1) / ppc);
-              if (k > n) k = n;
-              nv = SemWord::make(c, e + k, r);
-              mode = kAlloc;
-              arg = k;
-            } else if (c >= static_cast<long long>(n)) {
-              nv = SemWord::make(c - n, e, r);
-              mode = kTake;
-              arg = n;
-            } else {
-              nv = SemWord::make(c, e, r + n);
-              mode = kReserve;
-              arg = n;
-            }
-            unsigned long long seen = atomicCAS(&q->sem.v, v, nv);
-            if (seen == v) break;
-            if (tries > kSpinLimit) { note_timeout(h, kWaitSemCas); mode = kFail; break; }
-            // contended: back off before re-reading, so that thousands of
-            // arriving warps do not turn the word into a CAS storm
-            __nanosleep(16u << (tries < 6u ? tries : 6u));
-            v = ld_relaxed(&q->sem.v);
-          }
-          if (mode == kReserve) {
-            // wait until the pages are there or our reservation is no longer covered
-            uint32_t it = 0;
-            for (;;) {
-              unsigned long long w = ld_relaxed(&q->sem.v);
-              long long c = SemWord::count(w);
-              long long cover = c + static_cast<long long>(SemWord::exp_chunks(w)) * ppc;
-              if (c >= static_cast<long long>(n) || static_cast<long long>(SemWord::reserved(w)) >= cover) break;
-              if (it >= kSpinLimit) { note_timeout(h, kWaitSemReserve); break; }
-              backoff(it);
-            }
-            atomicAdd(&q->sem.v, SemWord::sub(0) - (static_cast<unsigned long long>(n) << SemWord::kResShift));
-          }
-        }
-      }
-    }
-    mode = bcast(g, mode);
-    arg = bcast(g, arg);
-    if (mode == kTake) return arg;
-    if (mode == kFail) return 0u;
-    if (mode == kAlloc) {
-      uint32_t got = grow(arg);
-      if (got < arg) failed_alloc = true;
-      failed_alloc = bcast(g, static_cast<uint32_t>(failed_alloc)) != 0u;
+  uint32_t k = 0, b = 0;
+  unsigned long long old = 0;
+  if (g.is_leader()) {
+    old = atomicAdd(&q->sem.v, SemWord::take(n));
+    const long long c0 = SemWord::count(old);
+    if (c0 < static_cast<long long>(n)) {
+      const uint32_t a = c0 < 0 ? static_cast<uint32_t>(-c0) : 0u;
+      b = static_cast<uint32_t>(static_cast<long long>(n) - c0);
+      k = (b + ppc - 1u) / ppc - (a + ppc - 1u) / ppc;   // multiples of ppc in [a, b)
+    } else if (SemWord::is_short(old)) {
+      sem_maybe_clear_short(q, old + SemWord::take(n));
     }
   }
+  k = bcast(g, k);
+  if (k) grow(k);
+  if (!bcast(g, b)) return n;
+  // In deficit: wait until supply has covered the slice, or resolve against
+  // what is there when an addition fell short.
+  uint32_t granted = n;
+  if (g.is_leader()) {
+    uint32_t it = 0;
+    for (;;) {
+      const unsigned long long w = ld_relaxed(&q->sem.v);
+      if (SemWord::supply_since(old, w) >= b) break;
+      if (SemWord::is_short(w)) {
+        const unsigned long long after = atomicAdd(&q->sem.v, SemWord::give(n));
+        sem_maybe_clear_short(q, after + SemWord::give(n));
+        granted = sem_take_upto(h, q, n);
+        break;
+      }
+      if (it >= kSpinLimit) {
+        note_timeout(h, kWaitSemReserve);
+        atomicAdd(&q->sem.v, SemWord::give(n));
+        granted = 0;
+        break;
+      }
+      backoff(it);
+    }
+  }
+  return bcast(g, granted);
 }
 
 }  // namespace ouro
