@@ -406,11 +406,15 @@ REF_ATOMICS_PER_PAIR = {"P": 2 + 4 / 32, "VAP": 4 + 4 / 32, "VLP": 4 + 4 / 32,
 
 def roofline(res, n, steps) -> dict:
     """Roofline of the dominant kernel: the (kernel, instantiation) pair with the
-    largest share of the timed kernel time.  Every warp group of a class
-    serialises on the class's hot lines, so the bound is L2 atomic throughput
-    on those lines: achieved = hot RMWs per launch / average launch time,
-    against the measured single-address atomic rate times the number of
-    distinct hot lines (2, or 1 for chunk free)."""
+    largest share of the timed kernel time.  The path is bound by L2 atomic
+    throughput.  achieved = the per-lane L2 atomics of the reference's algorithm
+    for one launch (per alloc+free pair: P 2 + 4/g, VAP and VLP 4 + 4/g,
+    chunk-based 4 + 2/g, g = 32 lanes per class group; half of it per launch)
+    over the average launch time; peak = the distinct-address atomic rate of
+    this GPU, measured live (every lane of all SMs, one atomicAdd each on an
+    L2-resident array).  Beside it: the rate on the lines every group of a
+    class serialises on (semaphore + ticket or cursor) against the measured
+    single-address rate, and the DRAM traffic of the kernel from ncu."""
     import ouroboros_b200 as ob
     per = {}
     for (v, size), (a, f, _, _) in res.items():
@@ -424,10 +428,9 @@ def roofline(res, n, steps) -> dict:
     kind = "page" if v in ("P", "VAP", "VLP") else "chunk"
     hot_lines = HOT_RMW[(kind, kern)]
     groups = n / 32.0
-    achieved = hot_lines * groups / (avg_ms * 1e-3) / 1e9
+    hot_achieved = hot_lines * groups / (avg_ms * 1e-3) / 1e9
     hot = ob.measure_atomics(1)
     distinct = ob.measure_atomics(0)
-    peak = hot_lines * hot
     vidx = VARIANTS.index(v)
     traffic, traffic_cell = None, None
     try:
@@ -441,21 +444,24 @@ def roofline(res, n, steps) -> dict:
         hbm_peak, hbm_source = float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
     else:
         hbm_peak, hbm_source = FALLBACK_HBM_GBS, "no MEASURED_PEAKS.json: 6.65 TB/s copy bandwidth (of fallback)"
-    ref_atomics = REF_ATOMICS_PER_PAIR[v] / 2.0 * n
+    atomics = REF_ATOMICS_PER_PAIR[v] / 2.0 * n
+    achieved = atomics / (avg_ms * 1e-3) / 1e9
     return {
         "bound": "l2_atomic", "kernel": f"k_{kern}<{vidx}> ({v})", "share": round(ms_sum / total, 4),
-        "achieved": round(achieved, 4), "peak": round(peak, 4), "unit": "G hot-line RMW/s",
-        "frac": round(achieved / peak, 4), "traffic": traffic,
+        "achieved": round(achieved, 4), "peak": round(distinct, 2), "unit": "G atomics/s",
+        "frac": round(achieved / distinct, 5), "traffic": traffic,
         "traffic_unit": "bytes per launch (dram read + write, ncu)", "traffic_cell": traffic_cell,
-        "peak_source": f"measured live by ouro_measure_atomics: one hot 32-bit address, one RMW per warp, "
-                       f"x{hot_lines} independent hot lines",
+        "algorithmic_atomics_per_launch": atomics,
+        "peak_source": "measured live by ouro_measure_atomics(0): distinct addresses, every lane of all SMs "
+                       "(builder-measured; the driver's peaks file has no atomic figure)",
         "avg_launch_ms": round(avg_ms, 5), "launches": launches,
-        "reference_model": {
-            "what": "per-lane L2 atomics of the reference's algorithm for this launch (half of an alloc+free pair)",
-            "atomics_per_launch": ref_atomics,
-            "achieved_gops": round(ref_atomics / (avg_ms * 1e-3) / 1e9, 3),
-            "peak_gops": round(distinct, 2), "peak_source": "measured live: distinct-address atomics, all SMs",
-            "frac": round(ref_atomics / (avg_ms * 1e-3) / 1e9 / distinct, 5)},
+        "hot_line": {
+            "what": "RMWs on the lines every group of the class serialises on (semaphore + front/back ticket or "
+                    "scan cursor), one per warp group",
+            "rmw_per_launch": hot_lines * groups, "achieved_gops": round(hot_achieved, 4),
+            "peak_gops": round(hot_lines * hot, 4),
+            "peak_source": f"measured live: one hot 32-bit address, one RMW per warp, x{hot_lines} independent lines",
+            "frac": round(hot_achieved / (hot_lines * hot), 4)},
         "hbm": {"bytes_per_launch": 16.0 * n, "achieved_gbs": round(16.0 * n / (avg_ms * 1e-3) / 1e9, 2),
                 "peak_gbs": hbm_peak, "peak_source": hbm_source,
                 "frac": round(16.0 * n / (avg_ms * 1e-3) / 1e9 / hbm_peak, 5),

@@ -41,7 +41,8 @@ typedef enum {
   OURO_ERR_CUDA = 2,     /* a CUDA runtime call failed                    */
   OURO_ERR_NOMEM = 3,    /* cudaMalloc of the heap failed                 */
   OURO_ERR_DEVICE = 4,   /* the device reported an allocator error flag   */
-  OURO_ERR_TOO_LARGE = 5 /* beyond the fixed scratch of a no-alloc entry  */
+  OURO_ERR_TOO_LARGE = 5, /* beyond the fixed scratch of a no-alloc entry */
+  OURO_ERR_FULL = 6       /* the serving loop's submission ring is full    */
 } ouro_status;
 
 /* Device-side error flags (ouro_heap_status.flags). */
@@ -85,10 +86,16 @@ int ouro_alloc(ouro_heap* h, uint32_t n, uint32_t size, const uint32_t* d_sizes,
 int ouro_free(ouro_heap* h, uint32_t n, void* const* d_ptrs, int block, void* stream);
 
 /* Sequential replay of an op trace by one GPU thread (threadIdx.x = tid,
- * blockIdx.x = bid) for parity with the reference.  ops[2i] = 0: malloc(ops[2i+1]);
- * 1: free(result of op ops[2i+1]).  results[i] (host array): class << 32 |
- * chunk << 9 | page, bit 63 = null, bit 62 = CUDA device heap; 0 for frees.
- * No counterpart in the reference, whose only caller is its benchmark. */
+ * blockIdx.x = bid) for parity with the reference.  Op kinds, ops[2i] with
+ * argument a = ops[2i+1]:
+ *   0: malloc(a);  1: free(the result of op a);
+ *   2: allocate_chunk();  3: enqueue_initial_chunk(a & 15, the chunk of op
+ *      a >> 14, (a >> 4) & 1023 available pages);  4: free page a & 1023 of the
+ *      chunk of op a >> 10.
+ * results[i] (host array): for mallocs class << 32 | chunk << 9 | page, bit 63 =
+ * null, bit 62 = CUDA device heap; for op 2 the chunk index; bit 63 for a failed
+ * op 2 or 3; otherwise 0.  No counterpart in the reference, whose only caller is
+ * its benchmark. */
 int ouro_trace(ouro_heap* h, const uint32_t* ops, uint64_t n_ops, uint64_t* results, uint32_t tid, uint32_t bid);
 
 /* The reference's updateMemoryManagerHost (include/device/Ouroboros_impl.cuh:137-144)
@@ -186,6 +193,31 @@ int ouro_check_heap(ouro_heap* h, ouro_heap_report* out);
  * 32 KiB (CUDA device heap) are refused.  Synchronizes `stream`. */
 int ouro_prefill(ouro_heap* h, uint64_t size, uint64_t pages, uint64_t* out_pages, void* stream);
 
+/* Ouroboros<...>::memory_manager.allocateChunk<false>  (include/device/Ouroboros.cuh:
+ * 108-136), the call a caller of enqueueInitialChunk makes first: one 8 KiB chunk
+ * of the heap (reuse queue first, then the bump pointer) into *out_chunk, or
+ * UINT32_MAX when none is left.  Its pages start at data_base + chunk x 8192
+ * (ouro_get_info).  Synchronous, default stream. */
+int ouro_allocate_chunk(ouro_heap* h, uint32_t* out_chunk);
+
+/* Ouroboros<...>::enqueueInitialChunk(queue_index, chunk_index, available_pages,
+ * pages_per_chunk)  (include/device/Ouroboros.cuh:291-295; PageQueue_impl.cuh:40-53,
+ * PageQueueVA_impl.cuh:94-125, PageQueueVL_impl.cuh:54-63, ChunkQueue_impl.cuh:
+ * 69-77, ChunkQueueVA_impl.cuh:54-72, ChunkQueueVL_impl.cuh:49-56), together with
+ * the chunk initializer its callers run first (PageIndexChunk.cuh:82-86,
+ * ChunkIndexChunk.cuh:73-78): chunk_index, from ouro_allocate_chunk, joins size
+ * class queue_index (0..9: 16 B << queue_index, the first instance, as in the
+ * reference) with its last available_pages pages free and the pages before them
+ * in the caller's use; they are freed like any page.  pages_per_chunk follows
+ * from the class (8192 / page size).  Page-based heaps queue the free pages in
+ * page order, chunk-based heaps queue the chunk; the class's semaphore gains
+ * available_pages.  The reference's standard and virtualized-array chunk queues
+ * accept this only as the class's first operation; here it may come at any
+ * time.  OURO_ERR_ARG for a class, chunk or page count out of range,
+ * OURO_ERR_DEVICE when the class's queue or the chunk budget has no room.
+ * Synchronous, default stream. */
+int ouro_enqueue_initial_chunk(ouro_heap* h, uint32_t queue_index, uint32_t chunk_index, uint32_t available_pages);
+
 /* The batched path (no counterpart in the reference, whose only caller is its
  * per-thread benchmark): persistent kernels serve n requests in tiles of
  * 4 x block; each tile is binned by size class in shared memory and served in
@@ -245,6 +277,59 @@ int ouro_graph_grow(ouro_heap* h, void** d_vptr, uint32_t* d_degree, const uint3
 int ouro_graph_check(void* const* d_vptr, const uint32_t* d_degree, const uint32_t* d_vertices, uint32_t n, uint32_t nv,
                      uint64_t seed, unsigned long long* d_out2, void* stream);
 int ouro_free_bytes_to(ouro_heap* h, unsigned long long* dst, void* stream);
+
+/* The serving loop (no counterpart in the reference; its consumer, ouroGraph,
+ * lives outside the reference tree): a persistent kernel that stays on the GPU
+ * and serves batches of graph-growth requests (ouro_graph_grow's work) that
+ * clients submit while it runs -- continuous batching without a host round
+ * trip per batch.
+ *   ouro_serve_start: launches the loop on its own non-blocking stream over the
+ *     graph (d_vptr / d_degree of ouro_graph_init).  Batches are taken in
+ *     submission order and admitted while the heap's free bytes, computed on
+ *     the device from allocator state, stay at or above watermark x heap bytes
+ *     (a batch is always admitted when none is in flight); at most
+ *     max_inflight batches run at once, split into tiles of 1,024 requests
+ *     that all blocks work on side by side.
+ *   ouro_serve_submit: one batch, n vertex ids already in device memory
+ *     (d_vertices stays valid until the batch is reported done).  A host store
+ *     into a pinned, mapped ring: no CUDA call.  OURO_ERR_FULL when `ring`
+ *     batches are submitted and not yet reported by ouro_serve_poll.
+ *   ouro_serve_poll: up to max finished batches into out (any order), with
+ *     device timestamps (%globaltimer, ns) taken when the loop saw the batch,
+ *     admitted it and finished it.  Never blocks.
+ *   ouro_serve_stop: no more submissions; waits until every submitted batch
+ *     is done and the kernel has returned.  OURO_ERR_DEVICE when the loop
+ *     ended on its own first (status: 1 = idle longer than idle_seconds).
+ *     Batches can still be polled afterwards.
+ *   ouro_serve_close: stops if needed and frees the loop's memory.
+ * While the loop runs it occupies every SM: calls that synchronize the device
+ * (ouro_state, ouro_check_heap, ...) wait for ouro_serve_stop. */
+typedef struct ouro_server ouro_server;
+typedef struct {
+  uint32_t ring;           /* submission ring: batches outstanding at once (default 4096)   */
+  uint32_t max_inflight;   /* batches admitted and unfinished at once (default 64)          */
+  int blocks_per_sm;       /* resident blocks of the loop per SM, 0: as many as fit          */
+  double watermark;        /* admission waits below this fraction of free heap (0.10)        */
+  double idle_seconds;     /* the loop returns after this long with nothing to do (10)       */
+} ouro_serve_config;
+typedef struct {
+  uint64_t seq;                 /* submission number, from 0                       */
+  uint32_t client, n;
+  uint64_t t_seen_ns, t_start_ns, t_done_ns;
+  uint64_t failed_allocs;       /* requests whose malloc returned nullptr           */
+  uint64_t lock_giveups;        /* requests that gave up waiting for their vertex   */
+  uint32_t held_back;           /* 1 when the watermark deferred its admission      */
+} ouro_serve_result;
+typedef struct {
+  uint64_t batches_seen, batches_admitted, held_back;
+  uint32_t status;
+} ouro_serve_stats;
+int ouro_serve_start(ouro_heap* h, void** d_vptr, uint32_t* d_degree, uint32_t nv, uint64_t seed,
+                     const ouro_serve_config* cfg, ouro_server** out);
+int ouro_serve_submit(ouro_server* s, const uint32_t* d_vertices, uint32_t n, uint32_t client, uint64_t* out_seq);
+int ouro_serve_poll(ouro_server* s, ouro_serve_result* out, uint32_t max, uint32_t* got);
+int ouro_serve_stop(ouro_server* s, ouro_serve_stats* out);
+int ouro_serve_close(ouro_server* s);
 
 /* Free resources of a heap (include/device/MemoryQueries.cuh:8-88
  * printFreeResources, include/device/Statistics.h:30-57), as numbers instead

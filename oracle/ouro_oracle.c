@@ -624,8 +624,9 @@ static int vl_enqueue(orc_heap* h, cq_t* q, uint32_t vpos, uint32_t element) {
   return ORC_OK;
 }
 
-/* QueueChunk_impl.cuh:189-319 linked enqueueChunk (SINGLE / V4 modes) */
-static int vl_enqueue_chunk(orc_heap* h, cq_t* q, uint32_t position, uint32_t c, uint32_t ppc) {
+/* QueueChunk_impl.cuh:189-319 linked enqueueChunk (SINGLE / V4 modes): ppc
+ * entries, pages start .. start + ppc - 1 of chunk c (its start_index) */
+static int vl_enqueue_chunk(orc_heap* h, cq_t* q, uint32_t position, uint32_t c, uint32_t ppc, uint32_t start) {
   chunk_t* k;
   uint32_t kidx;
   int rc = vl_locate(h, q->back_ptr, position, &k, &kidx);
@@ -645,7 +646,7 @@ static int vl_enqueue_chunk(orc_heap* h, cq_t* q, uint32_t position, uint32_t c,
   while (off < ppc) {
     if (local == 0u) k->next = potential_next;
     uint32_t step = v4 ? 4u : 1u;
-    for (uint32_t j = 0; j < step; ++j) k->slots[local + j] = mem_index(c, off + j);
+    for (uint32_t j = 0; j < step; ++j) k->slots[local + j] = mem_index(c, start + off + j);
     uint32_t old = k->qcount;
     k->qcount += (step << 16) + step;
     if ((old & 0xFFFFu) + step == QC_SPOTS) vl_set_back(h, q, kidx);
@@ -711,7 +712,7 @@ static int vlp_new_chunk(orc_heap* h, cq_t* q) {
   k->number_pages = q->ppc;
   uint32_t vpos = q->back;
   q->back += q->ppc;
-  rc = vl_enqueue_chunk(h, q, vpos, c, q->ppc);
+  rc = vl_enqueue_chunk(h, q, vpos, c, q->ppc, 0u);
   if (rc) return rc;
   sem_signal_expected(q, q->ppc);
   return ORC_OK;
@@ -1131,17 +1132,155 @@ int orc_free(orc_heap* h, uint64_t res) {
   }
 }
 
+/* Ouroboros.cuh:108-136 allocateChunk<false> of the first instance: the call a
+ * caller of enqueueInitialChunk makes first. */
+int orc_allocate_chunk(orc_heap* h, uint32_t* chunk) {
+  if (!h || !chunk) return ORC_ERR_ARG;
+  return allocate_chunk(h, 0, 0, chunk);
+}
+
+/* ChunkAccess.cuh:31-64: count = available pages, mask over number_pages with
+ * the first number_pages - available pages taken */
+static void access_init_avail(chunk_t* k, uint32_t available, uint32_t number_pages) {
+  k->acc_count = (int32_t)available;
+  k->acc_size = number_pages;
+  uint32_t taken = number_pages - available, n = number_pages;
+  for (int i = 0; i < 16; ++i) {
+    if (taken >= 32u) {
+      k->mask[i] = 0u;
+      taken -= 32u;
+    } else {
+      k->mask[i] = n >= 32u ? ~((1u << taken) - 1u) : (~((1u << taken) - 1u) & ((1u << n) - 1u));
+      taken = 0u;
+    }
+    n = n > 32u ? n - 32u : 0u;
+  }
+}
+
+/* Ouroboros.cuh:291-295 enqueueInitialChunk, after the chunk initializer its
+ * callers run (PageIndexChunk.cuh:82-86 / ChunkIndexChunk.cuh:73-78). */
+int orc_enqueue_initial(orc_heap* h, uint32_t queue_index, uint32_t c, uint32_t available) {
+  if (!h || queue_index >= (uint32_t)INST[0].nq) return ORC_ERR_ARG;
+  cq_t* q = &h->cq[0][queue_index];
+  if (available == 0u || available > q->ppc) return ORC_ERR_ARG;
+  chunk_t* k = chunk_at(h, c);
+  if (!k) return ORC_ERR_UB;
+  const uint32_t start = q->ppc - available;
+  k->page_size = INST[0].chunk_size / q->ppc;
+  int rc = ORC_OK;
+  if (h->page_based) {
+    k->number_pages = q->ppc;
+    if (h->kind == KIND_S) {
+      /* PageQueue_impl.cuh:40-53 */
+      for (uint32_t i = start; i < q->ppc; ++i) {
+        uint32_t* s = ring_slot(q, q->back++);
+        if (!s) return ORC_ERR_ARG;
+        *s = mem_index(c, i);
+      }
+    } else if (h->kind == KIND_VA) {
+      /* PageQueueVA_impl.cuh:94-125 */
+      for (uint32_t i = start; i < q->ppc; ++i) {
+        uint32_t vpos = q->back++;
+        uint32_t chunk_id = va_chunk_id(vpos);
+        if (vpos % QC_SPOTS == 0u) {
+          uint32_t nq;
+          rc = allocate_chunk(h, q->inst, 1, &nq);
+          if (rc) return rc;
+          rc = qc_init(h, nq, vpos + QC_SPOTS);
+          if (rc) return rc;
+          q->vq[(chunk_id + 1u) % VQ_SIZE] = nq;
+        }
+        chunk_t* qk;
+        rc = va_access(h, q, chunk_id, vpos, &qk);
+        if (rc) return rc;
+        qk->slots[vpos % QC_SPOTS] = mem_index(c, i);   /* QueueChunk_impl.cuh:77-83 enqueueInitial */
+        qk->qcount += (1u << 16) + 1u;
+      }
+    } else {
+      /* PageQueueVL_impl.cuh:54-63 */
+      uint32_t vpos = q->back;
+      q->back += available;
+      rc = vl_enqueue_chunk(h, q, vpos, c, available, start);
+      if (rc) return rc;
+    }
+  } else {
+    access_init_avail(k, available, q->ppc);
+    k->queue_pos = EMPTY32;
+    if (h->kind == KIND_S) {
+      /* ChunkQueue_impl.cuh:69-77: count_ is set, not raised */
+      q->count_ = 1;
+      uint32_t* s = ring_slot(q, q->back++);
+      if (!s) return ORC_ERR_ARG;
+      *s = c;
+    } else if (h->kind == KIND_VA) {
+      /* ChunkQueueVA_impl.cuh:54-72: the first entry of the first queue chunk,
+       * then the second queue chunk; defined only on a fresh queue */
+      if (q->back != 0u) return ORC_ERR_UB;
+      ++q->count_;
+      ++q->back;
+      chunk_t* qk;
+      rc = va_access(h, q, 0u, 0u, &qk);
+      if (rc) return rc;
+      qk->slots[0] = c;
+      qk->qcount += (1u << 16) + 1u;
+      uint32_t nq;
+      rc = allocate_chunk(h, q->inst, 1, &nq);
+      if (rc) return rc;
+      rc = qc_init(h, nq, QC_SPOTS);
+      if (rc) return rc;
+      q->vq[1] = nq;
+    } else {
+      /* ChunkQueueVL_impl.cuh:49-56 */
+      rc = vlc_enqueue(h, q, c);
+      if (rc) return rc;
+    }
+  }
+  sem_signal(q, available);
+  return ORC_OK;
+}
+
+/* The encoded result of page `page` of chunk c, for a free of a page that a
+ * caller held from an initial chunk. */
+static int page_result(orc_heap* h, uint32_t c, uint32_t page, uint64_t* res) {
+  chunk_t* k = chunk_at(h, c);
+  if (!k || k->page_size == 0u) return ORC_ERR_ARG;
+  int inst = k->page_size <= (INST[0].smallest << (INST[0].nq - 1)) ? 0 : 1;
+  int qi = queue_index(inst, k->page_size);
+  *res = ((uint64_t)(inst * 16 + qi) << 32) | (uint64_t)mem_index(c, page);
+  return ORC_OK;
+}
+
 int orc_run_trace(orc_heap* h, const uint32_t* ops, uint64_t n_ops, uint64_t* res, int64_t* ref_off,
                   uint64_t* failed_at) {
   if (!h || !ops || !res || !ref_off) return ORC_ERR_ARG;
   for (uint64_t i = 0; i < n_ops; ++i) {
     int rc;
-    if (ops[2 * i] == 0u) {
-      rc = orc_malloc(h, ops[2 * i + 1], &res[i], &ref_off[i]);
+    const uint32_t op = ops[2 * i], arg = ops[2 * i + 1];
+    res[i] = 0;
+    ref_off[i] = 0;
+    if (op == 0u) {
+      rc = orc_malloc(h, arg, &res[i], &ref_off[i]);
+    } else if (op == 1u) {
+      if (arg >= i || ops[2 * arg] != 0u) rc = ORC_ERR_ARG;
+      else rc = orc_free(h, res[arg]);
+    } else if (op == 2u) {
+      uint32_t c = 0;
+      rc = orc_allocate_chunk(h, &c);
+      res[i] = c;
+      ref_off[i] = c;
+    } else if (op == 3u || op == 4u) {
+      uint64_t j = op == 3u ? (arg >> 14) : (arg >> 10);
+      if (j >= i || ops[2 * j] != 2u) {
+        rc = ORC_ERR_ARG;
+      } else if (op == 3u) {
+        rc = orc_enqueue_initial(h, arg & 15u, (uint32_t)res[j], (arg >> 4) & 1023u);
+      } else {
+        uint64_t r = 0;
+        rc = page_result(h, (uint32_t)res[j], arg & 1023u, &r);
+        if (!rc) rc = orc_free(h, r);
+      }
     } else {
-      uint64_t j = ops[2 * i + 1];
-      if (j >= i || ops[2 * j] != 0u) { rc = ORC_ERR_ARG; }
-      else { rc = orc_free(h, res[j]); res[i] = 0; ref_off[i] = 0; }
+      rc = ORC_ERR_ARG;
     }
     if (rc) { if (failed_at) *failed_at = i; return rc; }
   }

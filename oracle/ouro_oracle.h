@@ -66,9 +66,19 @@ int orc_malloc(orc_heap* h, uint64_t size, uint64_t* res, int64_t* ref_off);
 /* One free of a result previously returned by orc_malloc. */
 int orc_free(orc_heap* h, uint64_t res);
 
-/* Trace replay.  ops[2i] = 0 -> malloc(ops[2i+1]); 1 -> free(result of op ops[2i+1]).
- * res[i] / ref_off[i] as for orc_malloc (0 for frees).  Stops at the first error
- * and reports the failing op index in *failed_at. */
+/* allocateChunk<false> of the first instance (Ouroboros.cuh:108-136). */
+int orc_allocate_chunk(orc_heap* h, uint32_t* chunk);
+/* enqueueInitialChunk (Ouroboros.cuh:291-295) of chunk c into class queue_index
+ * of the first instance, after the chunk initializer its callers run: the last
+ * `available` pages free, the ones before them in the caller's use. */
+int orc_enqueue_initial(orc_heap* h, uint32_t queue_index, uint32_t c, uint32_t available);
+
+/* Trace replay.  ops[2i] = 0 -> malloc(a); 1 -> free(result of op a);
+ * 2 -> allocate a chunk; 3 -> enqueue_initial(a & 15, chunk of op a >> 14,
+ * (a >> 4) & 1023 pages); 4 -> free page a & 1023 of the chunk of op a >> 10
+ * (a = ops[2i+1]).  res[i] / ref_off[i] as for orc_malloc, the chunk index for
+ * op 2, 0 otherwise.  Stops at the first error and reports the failing op index
+ * in *failed_at. */
 int orc_run_trace(orc_heap* h, const uint32_t* ops, uint64_t n_ops,
                   uint64_t* res, int64_t* ref_off, uint64_t* failed_at);
 

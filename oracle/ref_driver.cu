@@ -34,18 +34,39 @@ __global__ void k_trace(MM* mm, const uint32_t* ops, uint64_t n, int64_t* off, v
   char* d_data = reinterpret_cast<char*>(mm->memory.d_data);
   char* d_mem = reinterpret_cast<char*>(mm->memory.d_memory);
   size_t asz = mm->memory.allocationSize;
+  using ChunkType = typename MM::ChunkType;
   for (uint64_t i = 0; i < n; ++i) {
-    if (ops[2 * i] == 0u) {
-      void* p = mm->malloc(ops[2 * i + 1]);
+    const uint32_t op = ops[2 * i], arg = ops[2 * i + 1];
+    ptrs[i] = nullptr;
+    off[i] = 0;
+    if (op == 0u) {
+      void* p = mm->malloc(arg);
       ptrs[i] = p;
       char* c = reinterpret_cast<char*>(p);
       if (!p) off[i] = -1;
       else if (c > d_mem && c < d_mem + asz) off[i] = c - d_data;
       else off[i] = -2;
+    } else if (op == 1u) {
+      mm->free(ptrs[arg]);
+    } else if (op == 2u) {
+      // the first instance's allocateChunk (Ouroboros.cuh:108-136), as a
+      // caller of enqueueInitialChunk does before it
+      index_t c = 0;
+      mm->memory_manager.template allocateChunk<false>(c);
+      off[i] = c;
+    } else if (op == 3u) {
+      // chunk initializer (PageIndexChunk.cuh:82-86 / ChunkIndexChunk.cuh:73-78)
+      // then Ouroboros.cuh:291-295 enqueueInitialChunk
+      const index_t c = static_cast<index_t>(off[arg >> 14]);
+      const uint32_t qi = arg & 15u, avail = (arg >> 4) & 1023u, ppc = 512u >> qi;
+      ChunkType::initializeChunk(mm->memory.d_data, c, static_cast<int>(avail), ppc);
+      __threadfence();
+      mm->enqueueInitialChunk(qi, c, static_cast<int>(avail), ppc);
     } else {
-      mm->free(ptrs[ops[2 * i + 1]]);
-      ptrs[i] = nullptr;
-      off[i] = 0;
+      // free of a page the caller held from an initial chunk
+      const index_t c = static_cast<index_t>(off[arg >> 10]);
+      const unsigned int ps = ChunkType::getAccess(mm->memory.d_data, c)->page_size;
+      mm->free(ChunkType::getPage(mm->memory.d_data, c, arg & 1023u, ps));
     }
   }
 }

@@ -41,6 +41,8 @@ EXPORTS = (
     "ouro_status_string", "ouro_check_allocations_noalloc", "ouro_free_resources", "ouro_prefill",
     "ouro_alloc_batch", "ouro_free_batch", "ouro_realloc_batch", "ouro_autotune_batch",
     "ouro_graph_init", "ouro_graph_grow", "ouro_graph_check", "ouro_free_bytes_to",
+    "ouro_allocate_chunk", "ouro_enqueue_initial_chunk",
+    "ouro_serve_start", "ouro_serve_submit", "ouro_serve_poll", "ouro_serve_stop", "ouro_serve_close",
 )
 
 
@@ -80,6 +82,24 @@ class _HeapReport(ctypes.Structure):
                 ("sem_reserved", ctypes.c_uint64 * 12), ("data_chunks", ctypes.c_uint64), ("bad", ctypes.c_uint64)]
 
 
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("ring", ctypes.c_uint32), ("max_inflight", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_int),
+                ("watermark", ctypes.c_double), ("idle_seconds", ctypes.c_double)]
+
+
+class ServeResult(ctypes.Structure):
+    _fields_ = [("seq", ctypes.c_uint64), ("client", ctypes.c_uint32), ("n", ctypes.c_uint32),
+                ("t_seen_ns", ctypes.c_uint64), ("t_start_ns", ctypes.c_uint64), ("t_done_ns", ctypes.c_uint64),
+                ("failed_allocs", ctypes.c_uint64), ("lock_giveups", ctypes.c_uint64), ("held_back", ctypes.c_uint32)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("batches_seen", ctypes.c_uint64), ("batches_admitted", ctypes.c_uint64),
+                ("held_back", ctypes.c_uint64), ("status", ctypes.c_uint32)]
+
+
+OURO_ERR_FULL = 6
+
 _lib = None
 
 
@@ -110,6 +130,13 @@ def lib():
         L.ouro_check_allocations_noalloc.argtypes = [p, p, u32, u32, p, p, p]
         L.ouro_free_resources.argtypes = [p, ctypes.POINTER(_FreeReport)]
         L.ouro_prefill.argtypes = [p, u64, u64, ctypes.POINTER(ctypes.c_uint64), p]
+        L.ouro_allocate_chunk.argtypes = [p, ctypes.POINTER(ctypes.c_uint32)]
+        L.ouro_serve_start.argtypes = [p, p, p, u32, u64, ctypes.POINTER(ServeConfig), ctypes.POINTER(p)]
+        L.ouro_serve_submit.argtypes = [p, p, u32, u32, ctypes.POINTER(ctypes.c_uint64)]
+        L.ouro_serve_poll.argtypes = [p, ctypes.POINTER(ServeResult), u32, ctypes.POINTER(ctypes.c_uint32)]
+        L.ouro_serve_stop.argtypes = [p, ctypes.POINTER(ServeStats)]
+        L.ouro_serve_close.argtypes = [p]
+        L.ouro_enqueue_initial_chunk.argtypes = [p, u32, u32, u32]
         L.ouro_alloc_batch.argtypes = [p, p, p, u32, i, p]
         L.ouro_free_batch.argtypes = [p, p, u32, i, p]
         L.ouro_realloc_batch.argtypes = [p, p, p, u32, u64, u32, u32, ctypes.POINTER(_SizeDist), i, p]
@@ -202,6 +229,19 @@ class Ouroboros:
 
     def free(self, ptrs, n: int, block: int = 256, stream=None):
         _check(lib().ouro_free(self._handle(), n, _addr(ptrs), block, _stream(stream)), "ouro_free")
+
+    def allocate_chunk(self) -> int:
+        """allocateChunk<false> of the first instance (Ouroboros.cuh:108-136): an
+        8 KiB chunk index, or 0xFFFFFFFF when none is left."""
+        out = ctypes.c_uint32()
+        _check(lib().ouro_allocate_chunk(self._handle(), ctypes.byref(out)), "ouro_allocate_chunk")
+        return int(out.value)
+
+    def enqueue_initial_chunk(self, queue_index: int, chunk_index: int, available_pages: int):
+        """enqueueInitialChunk (Ouroboros.cuh:291-295): the chunk joins class
+        queue_index with its last available_pages pages free."""
+        _check(lib().ouro_enqueue_initial_chunk(self._handle(), queue_index, chunk_index, available_pages),
+               "ouro_enqueue_initial_chunk")
 
     def trace(self, ops: np.ndarray, tid: int = 0, bid: int = 0) -> np.ndarray:
         ops = np.ascontiguousarray(ops, dtype=np.uint32)

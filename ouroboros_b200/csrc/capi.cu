@@ -93,16 +93,40 @@ __global__ void k_trace(Ouroboros<V>* mm, const uint32_t* ops, uint64_t n, uint6
                         uint32_t bid) {
   if (threadIdx.x != tid || blockIdx.x != bid) return;
   for (uint64_t i = 0; i < n; ++i) {
-    if (ops[2 * i] == 0u) {
-      void* p = mm->malloc(ops[2 * i + 1]);
+    const uint32_t op = ops[2 * i], arg = ops[2 * i + 1];
+    ptrs[i] = nullptr;
+    res[i] = 0;
+    if (op == 0u) {
+      void* p = mm->malloc(arg);
       ptrs[i] = p;
       res[i] = encode_result(mm, p);
+    } else if (op == 1u) {
+      mm->free(ptrs[arg]);
+    } else if (op == 2u) {
+      const uint32_t c = mm->allocate_chunk();
+      res[i] = c == kEmpty ? (1ull << 63) : c;
+    } else if (op == 3u) {
+      const bool ok = mm->enqueue_initial_chunk(arg & 15u, static_cast<uint32_t>(res[arg >> 14]), (arg >> 4) & 1023u);
+      res[i] = ok ? 0ull : (1ull << 63);
     } else {
-      mm->free(ptrs[ops[2 * i + 1]]);
-      ptrs[i] = nullptr;
-      res[i] = 0;
+      const uint32_t c = static_cast<uint32_t>(res[arg >> 10]);
+      const uint32_t ps = ld_relaxed(&mm->meta[c].page_size);
+      mm->free(mm->data + (static_cast<size_t>(c) << kChunkShift) + static_cast<size_t>(arg & 1023u) * ps);
     }
   }
+}
+
+// One lane runs the reference's allocateChunk / enqueueInitialChunk for the
+// host (r: the chunk, or 1 for success).
+template <int V>
+__global__ void k_allocate_chunk(Ouroboros<V>* mm, unsigned long long* r) {
+  const uint32_t c = mm->allocate_chunk();
+  *r = c == kEmpty ? ~0ull : c;
+}
+template <int V>
+__global__ void k_enqueue_initial(Ouroboros<V>* mm, uint32_t queue_index, uint32_t chunk, uint32_t avail,
+                                  unsigned long long* r) {
+  *r = mm->enqueue_initial_chunk(queue_index, chunk, avail) ? 1ull : 0ull;
 }
 
 __device__ __forceinline__ uint32_t pattern_seed(uint32_t i, uint32_t seed) {
@@ -252,6 +276,7 @@ const char* ouro_status_string(int code) {
     case OURO_ERR_DEVICE: return "allocator reported an error on the device";
     case OURO_ERR_TOO_LARGE:
       return "heap too large for the fixed scratch of ouro_check_allocations_noalloc (at most 1 GiB of chunk data)";
+    case OURO_ERR_FULL: return "the serving loop's submission ring is full";
     default: return "unknown status";
   }
 }
@@ -405,9 +430,13 @@ int ouro_free(ouro_heap* h, uint32_t n, void* const* d_ptrs, int block, void* st
 int ouro_trace(ouro_heap* h, const uint32_t* ops, uint64_t n_ops, uint64_t* results, uint32_t tid, uint32_t bid) {
   if (!h || !ops || !results || n_ops == 0 || tid >= 1024u) return OURO_ERR_ARG;
   for (uint64_t i = 0; i < n_ops; ++i) {
-    // a free must name an earlier malloc
-    if (ops[2 * i] > 1u) return OURO_ERR_ARG;
-    if (ops[2 * i] == 1u && (ops[2 * i + 1] >= i || ops[2 * ops[2 * i + 1]] != 0u)) return OURO_ERR_ARG;
+    // a free must name an earlier malloc; an initial-chunk enqueue or a page
+    // free of such a chunk must name an earlier chunk allocation
+    const uint32_t op = ops[2 * i], arg = ops[2 * i + 1];
+    if (op > 4u) return OURO_ERR_ARG;
+    if (op == 1u && (arg >= i || ops[2 * arg] != 0u)) return OURO_ERR_ARG;
+    const uint64_t src = op == 3u ? (arg >> 14) : (arg >> 10);
+    if ((op == 3u || op == 4u) && (src >= i || ops[2 * src] != 2u)) return OURO_ERR_ARG;
   }
   uint32_t* d_ops = nullptr;
   uint64_t* d_res = nullptr;
@@ -457,7 +486,7 @@ int ouro_state(ouro_heap* h, uint64_t* out) {
     uint64_t* o = out + 7 + 12 * c;
     o[0] = static_cast<uint64_t>(SemWord::count(q.sem.v));
     o[1] = 0;   // expected and reserved pages of the reference's semaphore: none at quiescence
-    o[2] = SemWord::is_short(q.sem.v) ? 1u : 0u;
+    o[2] = q.holes > 0 ? static_cast<uint64_t>(q.holes) : 0u;
     o[3] = q.front.v;
     o[4] = q.back.v;
     o[5] = chunk_based && kind != 2 ? static_cast<uint64_t>(static_cast<int64_t>(q.entries.v)) : 0u;
@@ -569,7 +598,7 @@ int ouro_check_heap(ouro_heap* h, ouro_heap_report* out) {
     out->free_pages_meta[c] = chunk_based ? hr[12 + c] : static_cast<uint64_t>(q.back.v - q.front.v);
     out->sem_count[c] = SemWord::count(q.sem.v);
     out->sem_expected[c] = 0;   // no expected pages: groups in deficit own the chunks they add
-    out->sem_reserved[c] = SemWord::is_short(q.sem.v) ? 1u : 0u;   // an addition fell short, unresolved
+    out->sem_reserved[c] = 0;   // no reservations either: groups wait on supply
   }
   out->data_chunks = hr[24];
   out->bad = hr[25];
@@ -609,6 +638,39 @@ int ouro_prefill(ouro_heap* h, uint64_t size, uint64_t pages, uint64_t* out_page
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (out_pages) *out_pages = done * ppc;
   return cuda_rc(e);
+}
+
+int ouro_allocate_chunk(ouro_heap* h, uint32_t* out_chunk) {
+  if (!h || !out_chunk) return OURO_ERR_ARG;
+  unsigned long long* d_r = &h->dev->prefill_done.v;
+  dispatch(h->variant, [&](auto v) {
+    constexpr int V = decltype(v)::value;
+    k_allocate_chunk<V><<<1, 1>>>(reinterpret_cast<Ouroboros<V>*>(h->dev), d_r);
+    return 0;
+  });
+  unsigned long long r = ~0ull;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(&r, d_r, sizeof(r), cudaMemcpyDeviceToHost);
+  *out_chunk = r == ~0ull ? 0xFFFFFFFFu : static_cast<uint32_t>(r);
+  return cuda_rc(e);
+}
+
+int ouro_enqueue_initial_chunk(ouro_heap* h, uint32_t queue_index, uint32_t chunk_index, uint32_t available_pages) {
+  if (!h || queue_index >= 10u || chunk_index + 1ull >= h->L.max_chunks) return OURO_ERR_ARG;
+  const uint32_t ppc = class_pages_per_chunk(queue_index);
+  if (available_pages == 0u || available_pages > ppc) return OURO_ERR_ARG;
+  unsigned long long* d_r = &h->dev->prefill_done.v;
+  dispatch(h->variant, [&](auto v) {
+    constexpr int V = decltype(v)::value;
+    k_enqueue_initial<V><<<1, 1>>>(reinterpret_cast<Ouroboros<V>*>(h->dev), queue_index, chunk_index,
+                                   available_pages, d_r);
+    return 0;
+  });
+  unsigned long long r = 0;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(&r, d_r, sizeof(r), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return OURO_ERR_CUDA;
+  return r ? OURO_OK : OURO_ERR_DEVICE;
 }
 
 int ouro_free_resources(ouro_heap* h, ouro_free_report* out) {

@@ -48,6 +48,7 @@ struct alignas(128) ClassState {
   uint32_t class_chunks;          // chunk-based: chunks ever created for the class (budget)
   uint32_t page_cap;
   uint32_t clean_on_recycle;      // chunk queues: queue chunks hold kTomb entries when drained
+  int32_t holes;                  // semaphore: pages of failed chunk additions not yet handed back
   uint32_t* skip;                 // linked: index of recently linked queue chunks
   uint32_t* seg;                  // standard chunk queues: removed entries per 2048-entry ring segment
 };

@@ -55,6 +55,33 @@ struct Ouroboros : HeapCore {
     else return chunk_grow<Store>(this, q, g, k, false);
   }
 
+  // allocateChunk<false> of the first instance (Ouroboros.cuh:108-136), the
+  // call that callers of enqueueInitialChunk make first: one 8 KiB chunk from
+  // the reuse queue or the bump pointer, kEmpty when none is left.  One lane.
+  __device__ __forceinline__ uint32_t allocate_chunk() {
+    const Group self = make_group(1u << lane_id());
+    uint32_t c = kEmpty;
+    const uint32_t got = alloc_chunks(this, self, 1u, 0u, false, &c);
+    return got ? c : kEmpty;
+  }
+
+  // Ouroboros.cuh:291-295 enqueueInitialChunk(queue_index, chunk_index,
+  // available_pages, pages_per_chunk) with the chunk initializer its callers
+  // run before it: chunk `chunk` (from allocate_chunk) joins class
+  // queue_index (0..9, the first instance, as in the reference) with pages
+  // [ppc - available_pages, ppc) free and the pages before them in the
+  // caller's use (they are freed like any page); pages-per-chunk follows from
+  // the class.  One lane; false for bad arguments or when the class's queue or
+  // the chunk budget has no room.  The reference's standard and virtualized-
+  // array chunk queues accept it only as their class's first operation; here
+  // it may come at any time.
+  __device__ __forceinline__ bool enqueue_initial_chunk(uint32_t queue_index, uint32_t chunk, uint32_t available_pages) {
+    if (queue_index >= 10u) return false;
+    ClassState* q = &this->cls[queue_index];
+    if (available_pages == 0u || available_pages > q->ppc || chunk >= this->max_chunks - 1u) return false;
+    return enqueue_initial<Store, kPageBased>(this, q, chunk, available_pages);
+  }
+
   __device__ __forceinline__ void free(void* ptr) {
     const uint32_t active = __activemask();
     char* p = static_cast<char*>(ptr);

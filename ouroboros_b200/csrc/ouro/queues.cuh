@@ -121,7 +121,7 @@ __device__ uint32_t page_grow(HeapCore* h, ClassState* q, const Group& g, uint32
     __threadfence();
   }
   if (g.is_leader()) {
-    if (owed && got < k) sem_mark_short(q);
+    if (owed && got < k) sem_mark_short(q, (k - got) * q->ppc);
     sem_signal(q, E);
   }
   return got;
@@ -366,7 +366,7 @@ __device__ uint32_t chunk_grow(HeapCore* h, ClassState* q, const Group& g, uint3
   __syncwarp(g.mask);
   __threadfence();
   if (g.is_leader()) {
-    if (owed && got < k) sem_mark_short(q);
+    if (owed && got < k) sem_mark_short(q, (k - got) * q->ppc);
     sem_signal(q, got * q->ppc);
   }
   return got;
@@ -756,6 +756,68 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
   __threadfence();
   uint32_t total = __reduce_add_sync(g.mask, flashed ? 0u : 1u);
   if (g.is_leader()) sem_signal(q, total);
+}
+
+// ========================================================= initial chunks
+// Ouroboros.cuh:291-295 enqueueInitialChunk, together with the chunk
+// initializer its callers run first (PageIndexChunk.cuh:82-86,
+// ChunkIndexChunk.cuh:73-78 with ChunkAccess.cuh:31-64): chunk c, taken from
+// the pool by the caller, joins class q with its first ppc - avail pages in the
+// caller's use and the other avail pages free.  Page-based, those pages are
+// queued in page order (PageQueue_impl.cuh:40-53, PageQueueVA_impl.cuh:94-125,
+// PageQueueVL_impl.cuh:54-63); chunk-based, the chunk gets one queue entry
+// (ChunkQueue_impl.cuh:69-77, ChunkQueueVA_impl.cuh:54-72,
+// ChunkQueueVL_impl.cuh:49-56).  Then the semaphore gains avail pages.  One
+// lane; false when the queue or the chunk budget has no room.
+template <class Store, bool PageBased>
+__device__ bool enqueue_initial(HeapCore* h, ClassState* q, uint32_t c, uint32_t avail) {
+  const Group self = make_group(1u << lane_id());
+  const uint32_t ppc = q->ppc, start = ppc - avail;
+  ChunkMeta* m = h->meta + c;
+  if constexpr (PageBased) {
+    const uint32_t old = reserve_class_pages(h, q, ppc);
+    if (old == kEmpty) return false;
+    if constexpr (Store::kKind != 0) {
+      if (!commit_budget(h, 1u, 1u, old, ppc)) {
+        atomicSub(&q->class_pages, ppc);
+        return false;
+      }
+    }
+    init_data_chunk(h, q, c, false);
+    __threadfence();
+    const uint32_t b = atomicAdd(&q->back.v, avail);
+    Store::template publish_range<true>(h, q, self, b, avail, c, avail,
+                                        [start](uint32_t j, uint32_t cj) { return mem_index(cj, start + j); });
+    __threadfence();
+  } else {
+    if constexpr (Store::kKind != 0) {
+      const uint32_t old = atomicAdd(&q->class_chunks, 1u);
+      if (!commit_budget(h, 1u, 1u, 3u * old, 3u)) {
+        atomicSub(&q->class_chunks, 1u);
+        return false;
+      }
+    }
+    st_relaxed(&m->size, ppc);
+    st_relaxed(&m->head, 0u);
+    st_relaxed(&m->count, static_cast<int32_t>(avail));
+    st_relaxed(&m->queue_pos, kPending);
+    // ChunkAccess.cuh:31-64: pages [0, ppc - avail) taken, the rest free
+    uint32_t n = ppc, taken = start;
+#pragma unroll
+    for (uint32_t w = 0; w < 16u; ++w) {
+      const uint32_t full = n >= 32u ? 0xFFFFFFFFu : ((1u << n) - 1u);
+      const uint32_t used = taken >= 32u ? 0xFFFFFFFFu : ((1u << taken) - 1u);
+      st_relaxed(&m->mask[w], full & ~used);
+      n = n > 32u ? n - 32u : 0u;
+      taken = taken > 32u ? taken - 32u : 0u;
+    }
+    __threadfence();
+    st_relaxed(&m->page_size, q->page_size);
+    __threadfence();
+    chunk_enqueue<Store>(h, q, c);
+  }
+  sem_signal(q, avail);
+  return true;
 }
 
 }  // namespace ouro

@@ -5,9 +5,8 @@
 // and decides when chunks are added.  Its protocol is this build's own: a
 // group never loops on a CAS of the hot word.
 //
-//   word = count (bits 0..37, biased by 2^37) | short (bit 38) | supply
-//          (bits 39..63, pages ever added, mod 2^25; topmost, so that its
-//          carry leaves the word)
+//   word = count (bits 0..37, biased by 2^37) | supply (bits 38..63, pages
+//          ever added, mod 2^26; topmost, so that its carry leaves the word)
 //
 // * A group of n lanes takes n pages with ONE fetch-add of -n.  If the count
 //   before it was >= n the pages are there: done (the warm path).
@@ -21,13 +20,16 @@
 //   reference's decision, so sequential replays stay bit-exact with it.
 // * Adding pages (new chunks, frees, pre-fill) adds to count and supply in one
 //   fetch-add.  The pages of a group that went into deficit exist once supply
-//   has advanced by its slice end since its fetch-add; it waits for that
-//   (bounded) before it takes queue entries.
-// * Out of chunks: a failed addition sets `short` and adds only the pages it
-//   got.  Groups that still wait then see `short`, hand their demand back and
-//   take what is there with fetch-adds (take_upto), retrying while pages
-//   remain, so exactly the available pages are served and the rest get
-//   nullptr.  `short` is cleared once the count is back at or above zero.
+//   has advanced by its slice end since its fetch-add, or once the count is
+//   seen at or above zero; it waits for that (bounded) before it takes queue
+//   entries.
+// * Out of chunks: an addition that gets fewer chunks than it claimed adds the
+//   pages it got and records the missing ones as holes of the class.  While
+//   holes remain, waiting groups hand their demand back (paying holes down by
+//   as much) and take what is there with fetch-adds (take_upto), retrying
+//   while pages remain, so exactly the available pages are served and the
+//   rest get nullptr.  The unbacked part of the deficit never exceeds the
+//   holes, so a waiting group either sees its supply or sees holes.
 // * Every wait is bounded and reports a timeout instead of hanging.
 #pragma once
 
@@ -39,8 +41,7 @@ struct SemWord {
   static constexpr uint32_t kCntBits = 38u;
   static constexpr unsigned long long kCntMask = (1ull << kCntBits) - 1u;
   static constexpr unsigned long long kBias = 1ull << (kCntBits - 1u);
-  static constexpr unsigned long long kShort = 1ull << kCntBits;
-  static constexpr uint32_t kSupShift = kCntBits + 1u;
+  static constexpr uint32_t kSupShift = kCntBits;
   static constexpr uint32_t kSupBits = 64u - kSupShift;
   static constexpr unsigned long long kSupMask = (1ull << kSupBits) - 1u;
   static constexpr unsigned long long kInit = kBias;
@@ -51,7 +52,6 @@ struct SemWord {
   __host__ __device__ static uint32_t supply(unsigned long long v) {
     return static_cast<uint32_t>((v >> kSupShift) & kSupMask);
   }
-  __host__ __device__ static bool is_short(unsigned long long v) { return (v & kShort) != 0u; }
   // pages the supply field advanced from a to b (modular)
   __host__ __device__ static uint32_t supply_since(unsigned long long a, unsigned long long b) {
     return (supply(b) - supply(a)) & static_cast<uint32_t>(kSupMask);
@@ -65,27 +65,28 @@ struct SemWord {
   }
 };
 
-// `short` is cleared once nothing is owed.  Every operation that sees the
-// flag with the count (after the operation) at or above zero retries the
-// clear a few times; `now` is the word as that operation left it.
-__device__ __forceinline__ void sem_maybe_clear_short(ClassState* q, unsigned long long now) {
-  for (uint32_t tries = 0; tries < 8u && SemWord::is_short(now) && SemWord::count(now) >= 0; ++tries) {
-    const unsigned long long seen = atomicCAS(&q->sem.v, now, now & ~SemWord::kShort);
-    if (seen == now) return;
-    now = seen;
-  }
-}
-
 // Pages arrived (new chunks, a free, pre-fill): count += pages, supply += pages.
 __device__ __forceinline__ void sem_signal(ClassState* q, uint32_t pages) {
-  if (!pages) return;
-  const unsigned long long old = atomicAdd(&q->sem.v, SemWord::add(pages));
-  if (SemWord::is_short(old)) sem_maybe_clear_short(q, old + SemWord::add(pages));
+  if (pages) atomicAdd(&q->sem.v, SemWord::add(pages));
 }
 
-// An addition of chunks fell short of what the class owes: waiting groups
-// resolve their demand against the pages that are there.
-__device__ __forceinline__ void sem_mark_short(ClassState* q) { atomicOr(&q->sem.v, SemWord::kShort); }
+// An addition of chunks got `missing` pages fewer than it claimed.
+__device__ __forceinline__ void sem_mark_short(ClassState* q, uint32_t missing) {
+  if (missing) atomicAdd(&q->holes, static_cast<int32_t>(missing));
+}
+
+// A waiting group hands back its demand of n pages: holes go down by as much
+// (not below zero; a CAS loop, out-of-memory path only).
+__device__ __forceinline__ void sem_hand_back(ClassState* q, uint32_t n) {
+  atomicAdd(&q->sem.v, SemWord::give(n));
+  int32_t h = ld_relaxed(&q->holes);
+  for (uint32_t tries = 0; h > 0 && tries < 64u; ++tries) {
+    const int32_t nh = h > static_cast<int32_t>(n) ? h - static_cast<int32_t>(n) : 0;
+    const int32_t seen = atomicCAS(&q->holes, h, nh);
+    if (seen == h) break;
+    h = seen;
+  }
+}
 
 // BulkSemaphore_impl.cuh:7-17 tryReduce: take n pages only if all of them are
 // there.  Used by the standard chunk queue to hand a fully free chunk back to
@@ -116,7 +117,6 @@ __device__ inline uint32_t sem_take_upto(HeapCore* h, ClassState* q, uint32_t n)
     got += t;
     if (t == want) break;
     const unsigned long long now = atomicAdd(&q->sem.v, SemWord::give(want - t)) + SemWord::give(want - t);
-    sem_maybe_clear_short(q, now);
     if (SemWord::count(now) <= 0) break;
   }
   return got;
@@ -125,7 +125,7 @@ __device__ inline uint32_t sem_take_upto(HeapCore* h, ClassState* q, uint32_t n)
 // Acquire g.size pages of class q for the group.  Collective over the group;
 // the leader issues the atomics.  `grow(k)` is called collectively when the
 // group has to add k chunks; it publishes the pages it got, adds them with
-// sem_signal, and calls sem_mark_short if it got fewer than k chunks.
+// sem_signal, and calls sem_mark_short with the pages it did not get.
 // Returns the pages granted: g.size, or fewer when chunks ran out.
 template <typename Grow>
 __device__ inline uint32_t sem_acquire(HeapCore* h, ClassState* q, const Group& g, Grow&& grow) {
@@ -140,8 +140,6 @@ __device__ inline uint32_t sem_acquire(HeapCore* h, ClassState* q, const Group& 
       const uint32_t a = c0 < 0 ? static_cast<uint32_t>(-c0) : 0u;
       b = static_cast<uint32_t>(static_cast<long long>(n) - c0);
       k = (b + ppc - 1u) / ppc - (a + ppc - 1u) / ppc;   // multiples of ppc in [a, b)
-    } else if (SemWord::is_short(old)) {
-      sem_maybe_clear_short(q, old + SemWord::take(n));
     }
   }
   k = bcast(g, k);
@@ -153,11 +151,15 @@ __device__ inline uint32_t sem_acquire(HeapCore* h, ClassState* q, const Group& 
   if (g.is_leader()) {
     uint32_t it = 0;
     for (;;) {
+      // Covered once supply since the fetch-add reaches the slice end, or
+      // once the count is back at or above zero: then every demand made so
+      // far, this group's included, is backed by pages that are there (a
+      // group ahead that handed its demand back moved the slice forward
+      // without adding supply).
       const unsigned long long w = ld_relaxed(&q->sem.v);
-      if (SemWord::supply_since(old, w) >= b) break;
-      if (SemWord::is_short(w)) {
-        const unsigned long long after = atomicAdd(&q->sem.v, SemWord::give(n));
-        sem_maybe_clear_short(q, after + SemWord::give(n));
+      if (SemWord::supply_since(old, w) >= b || SemWord::count(w) >= 0) break;
+      if (ld_relaxed(&q->holes) > 0) {
+        sem_hand_back(q, n);
         granted = sem_take_upto(h, q, n);
         break;
       }

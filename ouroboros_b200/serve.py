@@ -1,26 +1,25 @@
 """Serving loop over the allocator: continuous batching of dynamic-graph growth.
 
 Clients send batches of vertex-growth requests (each request frees a vertex's
-edge block of 4 x d bytes and allocates one of 8 x d bytes, at most 8 KiB,
-through ``ouro_graph_grow``).  The state -- heap and graph -- stays on the
-device.  The scheduler admits batches as they arrive into a fixed number of
-stream slots, so batches that arrive while others run start as soon as a slot
-is free and their kernels overlap on the GPU; a client's next batch waits for
-its previous one.  Admission is deferred while the heap's free bytes -- read
-from allocator state by a small kernel on a side stream and copied to pinned
-host memory asynchronously, never synchronizing the device -- are below a
-watermark fraction of the heap.
-Latency of a batch = completion (its stream event seen done) - arrival.
+edge block of 4 x d bytes and allocates one of 8 x d bytes, at most 8 KiB).
+The state -- heap and graph -- stays on the device, and so does the loop: a
+persistent kernel (``ouro_serve_start``) takes batches from a ring in pinned,
+mapped host memory as clients submit them, admits them in arrival order while
+the heap's free bytes (computed on the device from allocator state) stay above
+a watermark fraction of the heap, and runs the tiles of every admitted batch
+side by side on all SMs.  Submitting is a host store, not a CUDA call.  This
+module is a thin client: it replays arrivals, submits, polls completions and
+reports latencies from the device's own timestamps (seen -> done).
 """
 from __future__ import annotations
 
-import collections
+import ctypes
 import time
 
 import numpy as np
 import torch
 
-from . import Ouroboros, _addr, _check, lib
+from . import OURO_ERR_FULL, Ouroboros, ServeConfig, ServeResult, ServeStats, _addr, _check, lib
 
 
 class Graph:
@@ -55,81 +54,112 @@ class Graph:
 
 
 class Server:
-    """Continuous batching of graph-growth batches into `slots` streams."""
+    """Client of the device-resident serving loop (ouro_serve_* of the C ABI)."""
 
-    def __init__(self, graph: Graph, slots: int = 16, watermark: float = 0.10):
-        self.g, self.slots, self.watermark = graph, int(slots), float(watermark)
-        self.streams = [torch.cuda.Stream() for _ in range(self.slots)]
-        self.query_stream = torch.cuda.Stream()
-        self.free_bytes_dev = torch.zeros(1, dtype=torch.int64, device="cuda")
-        self.free_bytes = torch.zeros(1, dtype=torch.int64).pin_memory()   # copied from the device, no sync
-        self.heap_bytes = graph.heap.info()["heap_bytes"]
+    def __init__(self, graph: Graph, max_inflight: int = 64, watermark: float = 0.10, ring: int = 4096,
+                 idle_seconds: float = 10.0, blocks_per_sm: int = 0):
+        self.g = graph
+        cfg = ServeConfig(int(ring), int(max_inflight), int(blocks_per_sm), float(watermark), float(idle_seconds))
+        h = ctypes.c_void_p()
+        _check(lib().ouro_serve_start(graph.heap._handle(), _addr(graph.vptr), _addr(graph.degree), graph.nv,
+                                      graph.seed, ctypes.byref(cfg), ctypes.byref(h)), "ouro_serve_start")
+        self._s = h
+        self._buf = (ServeResult * 1024)()
+        self._live = {}        # seq -> vertices tensor (kept alive until the batch is done)
+        self.done = []
+        self.stats = None
 
-    def _refresh_free_bytes(self):
-        _check(lib().ouro_free_bytes_to(self.g.heap._handle(), _addr(self.free_bytes_dev),
-                                        self.query_stream.cuda_stream), "ouro_free_bytes_to")
-        with torch.cuda.stream(self.query_stream):
-            self.free_bytes.copy_(self.free_bytes_dev, non_blocking=True)
+    def submit(self, vertices: torch.Tensor, client: int = 0):
+        """Submit one batch; returns its sequence number, or None when the ring is full."""
+        seq = ctypes.c_uint64()
+        rc = lib().ouro_serve_submit(self._s, _addr(vertices), vertices.numel(), int(client), ctypes.byref(seq))
+        if rc == OURO_ERR_FULL:
+            return None
+        _check(rc, "ouro_serve_submit")
+        self._live[int(seq.value)] = vertices
+        return int(seq.value)
+
+    def poll(self) -> int:
+        """Collect finished batches; returns how many came in."""
+        got = ctypes.c_uint32()
+        total = 0
+        while True:
+            _check(lib().ouro_serve_poll(self._s, self._buf, len(self._buf), ctypes.byref(got)), "ouro_serve_poll")
+            for i in range(got.value):
+                r = self._buf[i]
+                self._live.pop(int(r.seq), None)
+                self.done.append({f: getattr(r, f) for f, _ in ServeResult._fields_})
+            total += got.value
+            if got.value < len(self._buf):
+                return total
+
+    def stop(self) -> dict:
+        st = ServeStats()
+        rc = lib().ouro_serve_stop(self._s, ctypes.byref(st))
+        self.poll()
+        self.stats = {f: getattr(st, f) for f, _ in ServeStats._fields_}
+        if rc not in (0, 4):
+            _check(rc, "ouro_serve_stop")
+        return self.stats
+
+    def close(self):
+        if self._s:
+            lib().ouro_serve_close(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def run(self, batches, poll_s: float = 20e-6) -> dict:
         """batches: list of (arrival_s, client, vertices tensor on the device),
-        sorted by arrival.  Returns latencies and counters."""
-        pending = collections.deque()
-        arrivals = collections.deque(batches)
-        free_slots = list(range(self.slots))
-        busy_clients = set()
-        inflight = {}   # slot -> (event, arrival, client, requests)
-        lat, requests, deferred, peak = [], 0, 0, 0
-        self._refresh_free_bytes()
-        t0 = time.perf_counter()
-        while arrivals or pending or inflight:
-            now = time.perf_counter() - t0
-            while arrivals and arrivals[0][0] <= now:
-                pending.append(arrivals.popleft())
-            for slot, (ev, arr, client, nreq) in list(inflight.items()):
-                if ev.query():
-                    lat.append(time.perf_counter() - t0 - arr)
-                    requests += nreq
-                    busy_clients.discard(client)
-                    free_slots.append(slot)
-                    del inflight[slot]
-            self._refresh_free_bytes()
-            held = False
-            for _ in range(len(pending)):
-                if not free_slots:
-                    break
-                arr, client, verts = pending[0]
-                if client in busy_clients:   # a client's batches run in order
-                    pending.rotate(-1)
-                    continue
-                if int(self.free_bytes[0]) < self.watermark * self.heap_bytes:
-                    held = True
-                    break
-                pending.popleft()
-                slot = free_slots.pop()
-                st = self.streams[slot]
-                self.g.grow(verts, stream=st)
-                ev = torch.cuda.Event()
-                ev.record(st)
-                inflight[slot] = (ev, arr, client, verts.numel())
-                busy_clients.add(client)
-            deferred += int(held)
-            peak = max(peak, len(inflight))
-            if held and not inflight:
-                break   # the heap stays below the watermark: nothing in flight can free memory
-            if not inflight or not free_slots:
-                time.sleep(poll_s)
+        sorted by arrival (all at 0 for a saturating load).  Submits each at its
+        arrival time, polls completions meanwhile, stops after the last one and
+        reports latencies from the device timestamps (seen -> done)."""
         torch.cuda.synchronize()
+        requests = sum(int(b[2].numel()) for b in batches)
+        t0 = time.perf_counter()
+        full_waits = 0
+        for arr, client, verts in batches:
+            while time.perf_counter() - t0 < arr:
+                if not self.poll():
+                    time.sleep(poll_s)
+            while self.submit(verts, client) is None:
+                full_waits += 1
+                if not self.poll():
+                    time.sleep(poll_s)
+        deadline = time.perf_counter() + 120.0
+        while len(self.done) < len(batches) and time.perf_counter() < deadline:
+            if not self.poll():
+                time.sleep(poll_s)
+        stats = self.stop()
         wall = time.perf_counter() - t0
-        lat_ms = np.array(lat) * 1e3
-        failed = self.g.failed.tolist()
+        d = self.done
+        lat = np.array([(r["t_done_ns"] - r["t_seen_ns"]) * 1e-6 for r in d]) if d else np.zeros(0)
+        queue = np.array([(r["t_start_ns"] - r["t_seen_ns"]) * 1e-6 for r in d]) if d else np.zeros(0)
+        span_s = (max(r["t_done_ns"] for r in d) - min(r["t_seen_ns"] for r in d)) * 1e-9 if d else 0.0
+        done_requests = sum(r["n"] for r in d)
+        # batches running at once on the device: the most [start, done] intervals that overlap
+        ev = sorted([(r["t_start_ns"], 1) for r in d] + [(r["t_done_ns"], -1) for r in d])
+        peak = cur = 0
+        for _, step in ev:
+            cur += step
+            peak = max(peak, cur)
         return {
-            "batches": len(lat), "requests": requests, "wall_s": wall,
-            "ops_per_s": 2.0 * requests / wall,   # each request is one free and one malloc
-            "p50_ms": float(np.percentile(lat_ms, 50)) if len(lat) else None,
-            "p99_ms": float(np.percentile(lat_ms, 99)) if len(lat) else None,
-            "deferred_polls": deferred, "peak_inflight": peak, "left_pending": len(pending) + len(arrivals),
-            "failed_allocs": failed[0], "lock_giveups": failed[1],
+            "batches": len(d), "requests": done_requests, "wall_s": wall, "device_span_s": span_s,
+            "ops_per_s": 2.0 * done_requests / span_s if span_s > 0 else None,   # a request: one free, one malloc
+            "batches_per_s": len(d) / span_s if span_s > 0 else None,
+            "p50_ms": float(np.percentile(lat, 50)) if lat.size else None,
+            "p99_ms": float(np.percentile(lat, 99)) if lat.size else None,
+            "queue_p50_ms": float(np.percentile(queue, 50)) if queue.size else None,
+            "queue_p99_ms": float(np.percentile(queue, 99)) if queue.size else None,
+            "held_back": int(stats["held_back"]), "left_pending": len(batches) - len(d),
+            "ring_full_waits": full_waits, "loop_status": int(stats["status"]), "peak_inflight": peak,
+            "failed_allocs": int(sum(r["failed_allocs"] for r in d)),
+            "lock_giveups": int(sum(r["lock_giveups"] for r in d)),
+            "offered_requests": requests,
         }
 
 

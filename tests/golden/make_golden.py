@@ -7,7 +7,10 @@ The byte offsets it returns (page address minus the reference's d_data) and its
 counters after the trace are written to trace_<variant>.npz.  The reference has
 no tests or known-answer vectors of its own; these fixtures are its outputs.
 
-    python tests/golden/make_golden.py <out_dir>
+    python tests/golden/make_golden.py <out_dir> [trace names]
+
+With trace names, only those traces are run, and their arrays are added to the
+fixtures already in <out_dir> (the others are kept as they are).
 """
 from __future__ import annotations
 
@@ -29,11 +32,14 @@ def ops_digest(ops: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(ops, dtype=np.uint32).tobytes()).hexdigest()
 
 
-def main(out_dir: str) -> int:
+def main(out_dir: str, names=None) -> int:
     os.makedirs(out_dir, exist_ok=True)
-    built = {name: traces.build(name) for name in traces.TRACES}
+    built = {name: traces.build(name) for name in (names or traces.TRACES)}
     for v in oracle.VARIANTS:
         arrays = {}
+        path = os.path.join(out_dir, f"trace_{v}.npz")
+        if names and os.path.exists(path):
+            arrays.update(np.load(path))
         for name, (ops, tid, bid) in built.items():
             ref = oracle.RefDriver(v, traces.HEAP_BYTES)
             if "init_state" not in arrays:
@@ -51,4 +57,4 @@ def main(out_dir: str) -> int:
 
 
 if __name__ == "__main__":
-    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else HERE))
+    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else HERE, sys.argv[2:] or None))

@@ -1,7 +1,11 @@
 """Deterministic request traces for the sequential parity checks.
 
 A trace is a flat uint32 array of (kind, arg) pairs: kind 0 = malloc(arg bytes),
-kind 1 = free(the pointer returned by op number arg).  The same traces are
+kind 1 = free(the pointer returned by op number arg), kind 2 = take a chunk from
+the heap (the reference's allocateChunk), kind 3 = enqueue such a chunk as an
+initial chunk (the reference's enqueueInitialChunk; arg = op << 14 |
+available pages << 4 | queue index), kind 4 = free page (arg & 1023) of such a
+chunk (arg = op << 10 | page).  The same traces are
 replayed by one GPU thread through the reference build (make_golden.py), by the
 C oracle and by the CUDA allocator of this repository.  Every trace stays far
 from the heap's capacity and from the reference's queue limits, so that the
@@ -28,6 +32,17 @@ class _Builder:
     def free(self, i: int):
         self.ops += [1, int(i)]
         self.live.remove(i)
+
+    def alloc_chunk(self) -> int:
+        i = len(self.ops) // 2
+        self.ops += [2, 0]
+        return i
+
+    def enqueue_initial(self, chunk_op: int, queue_index: int, available: int):
+        self.ops += [3, (chunk_op << 14) | (available << 4) | queue_index]
+
+    def free_page(self, chunk_op: int, page: int):
+        self.ops += [4, (chunk_op << 10) | page]
 
     def free_all(self, order=None):
         for i in list(self.live if order is None else order):
@@ -112,6 +127,41 @@ def tier2() -> np.ndarray:
     return b.array()
 
 
+def initial() -> np.ndarray:
+    """Initial chunks (enqueueInitialChunk): on a fresh heap one chunk each for
+    64 B, 512 B and 2 KiB pages joins its class with its first pages in the
+    caller's use; mallocs take the initial pages first and then grow; the
+    caller's pages are freed along the way; everything freed at the end.  One
+    initial chunk per class: the reference's standard and virtualized-array
+    chunk queues accept it only as a class's first operation."""
+    b = _Builder()
+    c64, c512, c2k = b.alloc_chunk(), b.alloc_chunk(), b.alloc_chunk()
+    b.enqueue_initial(c64, 2, 125)     # pages 0..2 held by the caller
+    b.enqueue_initial(c512, 5, 10)     # pages 0..5 held
+    b.enqueue_initial(c2k, 7, 3)       # page 0 held
+    m64 = [b.malloc(64) for _ in range(200)]
+    m512 = [b.malloc(512) for _ in range(20)]
+    m2k = [b.malloc(2048) for _ in range(5)]
+    b.free_page(c64, 1)
+    b.free_page(c512, 0)
+    b.free_page(c512, 5)
+    b.free_page(c2k, 0)
+    for i in m64[::2]:
+        b.free(i)
+    for _ in range(50):
+        b.malloc(64)
+    b.free_page(c64, 0)
+    b.free_page(c64, 2)
+    for p in range(1, 5):
+        b.free_page(c512, p)
+    for i in m512[3:9] + m2k[1:3]:
+        b.free(i)
+    b.malloc(512)
+    b.malloc(2048)
+    b.free_all()
+    return b.array()
+
+
 # name -> (builder, tid, bid): the GPU thread that replays the trace
 TRACES = {
     "basic": (basic, 0, 0),
@@ -121,6 +171,7 @@ TRACES = {
     "churn512": (lambda: churn(512, 2500, 4), 0, 0),
     "chunk_fifo": (chunk_fifo, 0, 0),
     "tier2": (tier2, 0, 0),
+    "initial": (initial, 0, 0),
 }
 
 

@@ -46,3 +46,25 @@ def test_trace_matches_oracle(v, name):
     assert bad.size == 0, f"op {bad[0]}: got {oracle.decode(int(got[bad[0]]))} oracle {oracle.decode(int(want[bad[0]]))}"
     ost = o.state()
     assert np.array_equal(st, ost), _diff(st, ost)
+
+
+@pytest.mark.parametrize("v", ob.VARIANTS)
+def test_initial_chunk_entry_points_match_oracle(v):
+    # The host entry points (ouro_allocate_chunk, ouro_enqueue_initial_chunk)
+    # on a fresh heap, then a sequential trace: its mallocs take the initial
+    # pages first, in the oracle's order, and the counters agree.
+    with ob.Ouroboros(v, traces.HEAP_BYTES) as heap:
+        c = heap.allocate_chunk()
+        heap.enqueue_initial_chunk(3, c, 40)    # 128 B pages (64 a chunk): 24 held by the caller, 40 free
+        ops = np.array([0, 128] * 130, dtype=np.uint32)
+        got = heap.trace(ops)
+        st = heap.state()
+        with pytest.raises(ob.OuroError):
+            heap.enqueue_initial_chunk(3, c, 65)    # more pages than the chunk has
+    o = oracle.Oracle(v, traces.HEAP_BYTES)
+    oc = o.run_trace(np.array([2, 0, 3, (0 << 14) | (40 << 4) | 3], dtype=np.uint32))[0][0]
+    assert int(oc) == c
+    want, _ = o.run_trace(ops)
+    assert np.array_equal(got, want)
+    assert [oracle.decode(int(r))[2] for r in got[:3]] == [24, 25, 26]
+    assert np.array_equal(st, o.state()), _diff(st, o.state())
