@@ -68,8 +68,10 @@ def parse_args():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--no-churn", action="store_true", help="skip the churn measurement")
     ap.add_argument("--churn-rounds", type=int, default=1000)
-    ap.add_argument("--serving-seconds", type=float, default=1.0)
+    ap.add_argument("--serving-seconds", type=float, default=0.5)
     ap.add_argument("--no-config1", action="store_true", help="skip the 65,536 x 64 B page-based configuration")
+    ap.add_argument("--no-traces", action="store_true",
+                    help="skip the per-thread replays of the batched, churn and serving traces")
     return ap.parse_args()
 
 
@@ -158,6 +160,10 @@ class OursArm:
     def flags(self):
         return self.heap.status()["flags"]
 
+    def verify_nulls(self, ptrs, n, counters, stream):
+        # counters[0] += null pointers (size 0: no payload is read)
+        self.ob.verify_pattern(ptrs, n, counters, 0, SEED, None, stream)
+
     def detail(self) -> str:
         st = self.heap.status()
         return f"timeouts {st['timeouts']} at wait sites {st['timeout_sites']:#x}, nulls {st['null_results']}"
@@ -195,6 +201,9 @@ class ReferenceArm:
 
     def flags(self):
         return 0
+
+    def verify_nulls(self, ptrs, n, counters, stream):
+        self.oracle.ref_verify(ptrs.data_ptr(), n, 0, SEED, counters.data_ptr(), 0, stream.cuda_stream)
 
 
 class StdoutToStderr:
@@ -291,6 +300,212 @@ def run_cells(arm, cells, n, block, stream, ptrs, counters, flush, steps, warmup
               f"cold alloc {cold[0]:.4f} ms free {cold[1]:.4f} ms ({time.perf_counter() - t0:.2f}s)",
               file=sys.stderr, flush=True)
     return res
+
+
+def size_classes(sizes: np.ndarray) -> np.ndarray:
+    """Queue index of each request size (Helper.cuh:42-45): max(ceil_log2(size) - 4, 0), sizes <= 8 KiB."""
+    s = np.maximum(sizes.astype(np.int64), 1)
+    return np.maximum(np.ceil(np.log2(s)).astype(np.int64) - 4, 0)
+
+
+def chunks_for(class_pages: np.ndarray) -> int:
+    """Base chunks a set of live pages per class (first instance) needs: ceil(pages / pages-per-chunk)."""
+    ppc = 512 >> np.arange(10)
+    return int(np.sum(-(-class_pages // ppc)))
+
+
+def trace_configs(arm_cls, stream, is_reference: bool, churn_rounds: int = 10, serve_seconds: float = 0.25) -> dict:
+    """The batched, churn and serving configurations replayed through the plain
+    per-thread path (one launch of n threads for the allocations, one for the
+    frees, as src/main.cu does), with the same seeded traces for both arms:
+      batched_trace: VAC 8 GiB, 2^22 sizes log-uniform in [16, 8192] rounded
+        up to 16 B; a cold repetition then 3 warm ones (alloc all, free all);
+      churn_trace: VLC 16 GiB, a live set of 2^21 Zipf(1.2) sizes over the ten
+        16 B .. 8 KiB classes, then `churn_rounds` rounds, each freeing a
+        seeded 30% and allocating replacements;
+      serving_trace: VAP 32 GiB, the allocation trace of the serving workload
+        -- a 10M-vertex power-law graph's edge blocks (4 x degree bytes), then
+        `serve_seconds` of its batches (2,000 batches/s, 1k..256k requests
+        log-uniform, a batch's distinct vertices), each batch one launch that
+        allocates the doubled blocks (8 x degree bytes, at most 8 KiB) and one
+        that frees the old ones.
+    Only the allocation and free launches are timed (CUDA events, L2 flushed
+    before each launch of the batched trace).  The reference is run only where
+    a capacity model of the trace says it stays below maxChunks (its behaviour
+    past that is undefined)."""
+    import oracle
+    out = {}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    flush = torch.zeros(64 << 20, dtype=torch.int32, device="cuda")
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            ev[0].record(stream)
+            fn()
+            ev[1].record(stream)
+        stream.synchronize()
+        return ev[0].elapsed_time(ev[1])
+
+    # ---------------------------------------------------------------- batched
+    n = 1 << 22
+    rng = np.random.default_rng(2024)
+    sizes_np = (np.ceil(np.exp(rng.uniform(np.log(16), np.log(8192), n)) / 16) * 16).astype(np.uint32)
+    cls = size_classes(sizes_np)
+    need = chunks_for(np.bincount(cls, minlength=10)) + 12 * 8 + (3 * n) // 2048
+    mc = oracle.layout("VAC", 8 * GiB)["max_chunks"]
+    rec = {"workload": "VAC 8 GiB, 2^22 requests log-uniform 16..8192 B (rounded up to 16 B), per-thread alloc "
+                       "launch + free launch", "chunks_needed": need, "max_chunks": mc}
+    if is_reference and need + 1024 >= mc:
+        rec["skipped"] = "capacity model: the trace needs %d of %d chunks" % (need, mc)
+    else:
+        arm = arm_cls(8 * GiB)
+        sizes_d = torch.from_numpy(sizes_np.view(np.int32)).cuda()
+        ptrs = torch.zeros(n, dtype=torch.int64, device="cuda")
+        cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+        ms = []
+        with StdoutToStderr():
+            arm.open("VAC")
+            try:
+                for rep in range(4):
+                    flush.add_(1)
+                    a = timed(lambda: arm.alloc(n, 0, ptrs, 256, stream, sizes=sizes_d))
+                    if rep == 0:
+                        cnt.zero_()
+                        arm.verify_nulls(ptrs, n, cnt, stream)
+                    flush.add_(1)
+                    f = timed(lambda: arm.free(n, ptrs, 256, stream))
+                    ms.append((a, f))
+                flags = arm.flags()
+            finally:
+                arm.close()
+        warm = float(np.mean([a + f for a, f in ms[1:]]))
+        rec.update({"cold_mops": round(2.0 * n / ((ms[0][0] + ms[0][1]) * 1e-3) / 1e6, 2),
+                    "warm_mops": round(2.0 * n / (warm * 1e-3) / 1e6, 2),
+                    "cold_ms": [round(ms[0][0], 3), round(ms[0][1], 3)],
+                    "warm_ms": [round(float(np.mean([a for a, _ in ms[1:]])), 3),
+                                round(float(np.mean([f for _, f in ms[1:]])), 3)],
+                    "null_results_first_rep": int(cnt[0].item()), "flags": flags})
+    out["batched_trace"] = rec
+
+    # ------------------------------------------------------------------ churn
+    n = 1 << 21
+    rng = np.random.default_rng(99)
+    w = 1.0 / np.arange(1, 11) ** 1.2
+    w /= w.sum()
+    live_cls = rng.choice(10, size=n, p=w)
+    rounds_sizes, rounds_idx = [], []
+    for r in range(churn_rounds):
+        idx = np.nonzero(rng.random(n) < 0.3)[0]
+        rounds_idx.append(idx)
+        rounds_sizes.append(rng.choice(10, size=idx.size, p=w))
+    # capacity: live pages per class at their peak (allocations of a round come before nothing is freed? frees first)
+    peak = np.bincount(live_cls, minlength=10).astype(np.int64)
+    cur_cls = live_cls.copy()
+    for idx, new in zip(rounds_idx, rounds_sizes):
+        cur_cls[idx] = new
+        peak = np.maximum(peak, np.bincount(cur_cls, minlength=10))
+    need = chunks_for(peak) * 2 + 12 * 16
+    mc = oracle.layout("VLC", 16 * GiB)["max_chunks"]
+    rec = {"workload": "VLC 16 GiB, live set 2^21 Zipf(1.2) over 16 B..8 KiB, %d rounds of 30%% free + "
+                       "re-allocation, per-thread free launch + alloc launch" % churn_rounds,
+           "chunks_needed_bound": need, "max_chunks": mc}
+    if is_reference and need + 1024 >= mc:
+        rec["skipped"] = "capacity model: the trace may need %d of %d chunks" % (need, mc)
+    else:
+        arm = arm_cls(16 * GiB)
+        ptrs = torch.zeros(n, dtype=torch.int64, device="cuda")
+        sizes_d = torch.from_numpy((16 << live_cls).astype(np.uint32).view(np.int32)).cuda()
+        ms, ops = 0.0, 0
+        with StdoutToStderr():
+            arm.open("VLC")
+            try:
+                timed(lambda: arm.alloc(n, 0, ptrs, 256, stream, sizes=sizes_d))
+                for idx, new in zip(rounds_idx, rounds_sizes):
+                    m = idx.size
+                    idx_d = torch.from_numpy(idx).cuda()
+                    sub = ptrs[idx_d].contiguous()
+                    nsz = torch.from_numpy((16 << new).astype(np.uint32).view(np.int32)).cuda()
+                    ms += timed(lambda: arm.free(m, sub, 256, stream))
+                    ms += timed(lambda: arm.alloc(m, 0, sub, 256, stream, sizes=nsz))
+                    ptrs[idx_d] = sub
+                    ops += 2 * m
+                flags = arm.flags()
+            finally:
+                arm.close()
+        rec.update({"mops": round(ops / (ms * 1e-3) / 1e6, 2), "ms": round(ms, 3), "ops": ops, "flags": flags})
+    out["churn_trace"] = rec
+
+    # ---------------------------------------------------------------- serving
+    nv = 10_000_000
+    rng = np.random.default_rng(17)
+    u = rng.random(nv)
+    deg = np.minimum(np.maximum(np.floor(u ** (-1.0 / 1.1)), 1), 1024).astype(np.int64)   # P(d) ~ d^-2.1
+    batches = []
+    t, rate, clients = 0.0, 2000.0, 256
+    arr = []
+    for c in range(clients):
+        tt = 0.0
+        while True:
+            tt += rng.exponential(clients / rate)
+            if tt >= serve_seconds:
+                break
+            arr.append((tt, int(np.exp(rng.uniform(np.log(1000), np.log(256000))))))
+    arr.sort()
+    for _, size in arr:
+        batches.append(np.unique(rng.integers(0, nv, size)))
+    # capacity: page-based classes keep their chunks; live pages per class after each batch's allocations
+    cur = deg.copy()
+    cls_of = lambda d: size_classes(np.minimum(4 * d, 8192))
+    live = np.bincount(cls_of(cur), minlength=10).astype(np.int64)
+    peak = live.copy()
+    for v in batches:
+        d = cur[v]
+        g = v[d < 2048]
+        nd = np.minimum(2 * cur[g], 2048)
+        live_with_new = live + np.bincount(cls_of(nd), minlength=10)
+        peak = np.maximum(peak, live_with_new)
+        live = live_with_new - np.bincount(cls_of(cur[g]), minlength=10)
+        cur[g] = nd
+    need = chunks_for(peak) + sum(int(-(-p // 2048)) for p in peak) + 12 * 8
+    mc = oracle.layout("VAP", 32 * GiB)["max_chunks"]
+    rec = {"workload": "VAP 32 GiB, 10M-vertex power-law graph (alpha 2.1) edge blocks, then %.2f s of serving "
+                       "batches at 2,000 batches/s (%d batches, distinct vertices per batch): per batch one alloc "
+                       "launch (8 x degree bytes, at most 8 KiB) and one free launch of the old blocks"
+                       % (serve_seconds, len(batches)), "chunks_needed": need, "max_chunks": mc}
+    if is_reference and need + 1024 >= mc:
+        rec["skipped"] = "capacity model: the trace needs %d of %d chunks" % (need, mc)
+    else:
+        arm = arm_cls(32 * GiB)
+        vptr = torch.zeros(nv, dtype=torch.int64, device="cuda")
+        degree = torch.from_numpy(deg).cuda()
+        ms, ops = 0.0, 0
+        with StdoutToStderr():
+            arm.open("VAP")
+            try:
+                sz = (4 * degree).to(torch.int32)
+                timed(lambda: arm.alloc(nv, 0, vptr, 256, stream, sizes=sz))
+                for v in batches:
+                    vd = torch.from_numpy(v).cuda()
+                    d = degree[vd]
+                    vd = vd[d < 2048]
+                    m = int(vd.numel())
+                    if m == 0:
+                        continue
+                    nd = torch.clamp(2 * degree[vd], max=2048)
+                    nsz = (4 * nd).to(torch.int32)
+                    newp = torch.zeros(m, dtype=torch.int64, device="cuda")
+                    old = vptr[vd].contiguous()
+                    ms += timed(lambda: arm.alloc(m, 0, newp, 256, stream, sizes=nsz))
+                    ms += timed(lambda: arm.free(m, old, 256, stream))
+                    vptr[vd] = newp
+                    degree[vd] = nd
+                    ops += 2 * m
+                flags = arm.flags()
+            finally:
+                arm.close()
+        rec.update({"mops": round(ops / (ms * 1e-3) / 1e6, 2), "ms": round(ms, 3), "ops": ops, "flags": flags})
+    out["serving_trace"] = rec
+    return out
 
 
 def cold_summary(res, n) -> dict:
@@ -605,28 +820,50 @@ def churn_bench(rounds: int, stream) -> dict:
 def serving_bench(seconds: float) -> dict:
     """The serving configuration: page-based virtualized-array heap of 32 GiB
     holding a 10M-vertex power-law graph (degree exponent 2.1, uint32 ids);
-    256 clients with Poisson arrivals, 2,000 batches/s in total; batch sizes
-    log-uniform in 1k..256k requests, each request moving a vertex's edge
-    block from 4 x d to 8 x d bytes (at most 8 KiB); admission deferred while
-    free bytes are below 10% of the heap; continuous batching into 16 stream
-    slots.  `seconds` of arrivals."""
+    256 clients with Poisson arrivals; batch sizes log-uniform in 1k..256k
+    requests, each request moving a vertex's edge block from 4 x d to 8 x d
+    bytes (at most 8 KiB); admission deferred while free bytes are below 10%
+    of the heap.  Served by the device-resident loop (ouro_serve_*): three
+    rows, each on a fresh heap and graph with `seconds` of arrivals --
+    saturation (every batch at t = 0: the service rate), the configured
+    2,000 batches/s, and 80% of the measured service rate.  Latency = device
+    time from the loop seeing a batch to its last request done."""
     from ouroboros_b200 import serve
     import ouroboros_b200 as ob
     nv = 10_000_000
-    with ob.Ouroboros("VAP", 32 * GiB) as heap:
-        g = serve.Graph(heap, nv, seed=17, alpha=2.1)
-        batches = serve.poisson_batches(256, 2000.0, seconds, nv, 1000, 256_000, seed=23)
-        srv = serve.Server(g, slots=16, watermark=0.10)
-        rep = srv.run(batches)
-        rep["free_bytes_after"] = heap.free_resources()["free_bytes"]
-        rep["flags"] = heap.status()["flags"]
-    rep["workload"] = ("VAP 32 GiB, 10M-vertex power-law graph (alpha 2.1), 256 Poisson clients at 2000 batches/s, "
-                       "batches of 1k-256k growth requests (log-uniform), %.1f s of arrivals, 16 slots, "
-                       "10%% free-byte watermark" % seconds)
-    for k in ("wall_s", "ops_per_s", "p50_ms", "p99_ms"):
-        if rep.get(k) is not None:
-            rep[k] = round(rep[k], 3)
-    return rep
+    rows = {}
+
+    def one(name, rate, seed, at_zero=False):
+        with ob.Ouroboros("VAP", 32 * GiB) as heap:
+            g = serve.Graph(heap, nv, seed=17, alpha=2.1)
+            batches = serve.poisson_batches(256, rate, seconds, nv, 1000, 256_000, seed=seed)
+            if at_zero:
+                batches = [(0.0, c, v) for (_, c, v) in batches]
+            srv = serve.Server(g, max_inflight=64, watermark=0.10)
+            try:
+                rep = srv.run(batches)
+            finally:
+                srv.close()
+            rep["offered_batches_per_s"] = None if at_zero else rate
+            rep["free_bytes_after"] = heap.free_resources()["free_bytes"]
+            rep["flags"] = heap.status()["flags"]
+        for k in list(rep):
+            if isinstance(rep[k], float):
+                rep[k] = round(rep[k], 4)
+        rows[name] = rep
+        return rep
+
+    sat = one("saturated", 2000.0, 23, at_zero=True)
+    one("rate_2000", 2000.0, 23)
+    service = sat.get("batches_per_s") or 0.0
+    if service > 0:
+        one("rate_80pct_of_service", 0.8 * service, 29)
+    return {"workload": ("VAP 32 GiB, 10M-vertex power-law graph (alpha 2.1), 256 Poisson clients, batches of "
+                         "1k-256k growth requests (log-uniform), %.2f s of arrivals per row, device-resident loop "
+                         "(64 batches in flight at most), 10%% free-byte watermark; fresh heap and graph per row"
+                         % seconds),
+            "service_batches_per_s": round(service, 1) if service else None,
+            "rows": rows}
 
 
 # Copy bandwidth measured earlier on B200s of the same kind, used when no
@@ -761,6 +998,12 @@ def main():
             out["config1"] = config1_bench(ReferenceArm if args.impl == "reference" else OursArm, stream)
         except Exception as exc:   # reported, the headline stands
             out["config1"] = {"error": str(exc)[:300]}
+    if rank == 0 and not args.no_traces:
+        try:
+            out["per_thread_traces"] = trace_configs(ReferenceArm if args.impl == "reference" else OursArm, stream,
+                                                     args.impl == "reference")
+        except Exception as exc:   # reported, the headline stands
+            out["per_thread_traces"] = {"error": str(exc)[:300]}
     if args.impl == "reference":
         out["impl"] = "reference"
         out["gpu_launches"] = 0

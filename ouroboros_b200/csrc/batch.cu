@@ -4,14 +4,17 @@
 //
 // The per-thread path forms warp groups from whatever sizes a warp's 32
 // threads happen to ask for; with mixed sizes that is ~10 classes per warp,
-// so every class's semaphore and ticket atomics are issued by groups of ~3
-// lanes.  Here each block takes tiles of 4 x blockDim requests, bins them by
-// size class in shared memory (a histogram, a prefix sum and a scatter of
-// request indices), and serves the tile in binned order: consecutive lanes
-// of a warp then ask for the same class, and a warp's 32 requests cost one
-// semaphore and one ticket atomic.  Tiles are taken grid-stride by a
-// persistent grid (no counter to reset, so launches can be captured in CUDA
-// graphs).  Frees are binned by the class of the page they release.
+// so every class's semaphore and queue atomics are issued by groups of ~3
+// lanes.  Here every warp takes tiles of 1,024 requests (32 per lane),
+// counting-sorts the tile by size class in its own part of shared memory (a
+// histogram and a scatter of request indices, match_any-ranked, no block
+// barrier), and serves it in sorted order: the 32 lanes of a round then ask
+// for one class (two at a class boundary), so a round costs one semaphore and
+// one queue reservation instead of ten.  Warps never wait for each other: a
+// warp whose tile holds the slow large classes does not hold up the others.
+// Tiles are taken grid-stride by a persistent grid (no counter to reset, so
+// launches can be captured in CUDA graphs).  Frees are sorted by the class of
+// the page they release.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -22,8 +25,10 @@ using namespace ouro;
 
 namespace {
 
-constexpr int kPer = 4;                        // requests per thread and tile
 constexpr uint32_t kBins = kNumClasses + 1u;   // + the CUDA device heap
+constexpr uint32_t kNone = 15u;                // a slot without a request
+constexpr uint32_t kLaneSlots = 32u;           // requests per lane and tile
+constexpr uint32_t kWarpTile = 32u * kLaneSlots;
 
 __device__ __forceinline__ uint32_t bin_of_size(uint64_t size) {
   const int c = size_class(size);
@@ -41,74 +46,100 @@ __device__ __forceinline__ uint32_t bin_of_ptr(const Ouroboros<V>* mm, const voi
   return cls < 0 ? kNumClasses : static_cast<uint32_t>(cls);
 }
 
-// Shared-memory binning of one tile.  bins[j] is the bin of the thread's j-th
-// request (kBins: none); the request indices come out in `order`, grouped by
-// bin.  Returns the tile's request count.
-template <int BLOCK>
-__device__ __forceinline__ void bin_tile(const uint32_t (&bins)[kPer], const uint32_t (&req)[kPer], uint32_t* hist,
-                                         uint32_t* off, uint32_t* order) {
-  uint32_t slot[kPer];
-  if (threadIdx.x < kBins) hist[threadIdx.x] = 0;
-  __syncthreads();
+// Shared memory of one warp: the sorted slot indices of its tile and the
+// running offsets per bin.
+struct WarpBins {
+  uint16_t idx[kWarpTile];
+  uint32_t cur[16];
+};
+
+// Counting sort of the warp's tile slots by key (key[j] of this lane's slot
+// j, slot number j x 32 + lane; kNone: no request).  Writes the slot numbers
+// grouped by key into w.idx and returns how many there are.  Ranks come from
+// match_any, so the order within a key is the slot order.
+__device__ __forceinline__ uint32_t warp_bin(WarpBins& w, const uint8_t (&key)[kLaneSlots]) {
+  const uint32_t lane = lane_id();
+  const uint32_t lt = (1u << lane) - 1u;
+  if (lane < 16u) w.cur[lane] = 0;
+  __syncwarp();
 #pragma unroll
-  for (int j = 0; j < kPer; ++j) slot[j] = bins[j] < kBins ? atomicAdd(&hist[bins[j]], 1u) : 0u;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t acc = 0;
-    for (uint32_t b = 0; b < kBins; ++b) {
-      off[b] = acc;
-      acc += hist[b];
-    }
-    off[kBins] = acc;
+  for (uint32_t j = 0; j < kLaneSlots; ++j) {
+    const uint32_t m = __match_any_sync(0xFFFFFFFFu, key[j]);
+    if ((m & lt) == 0u && key[j] != kNone) w.cur[key[j]] += __popc(m);
+    __syncwarp();
   }
-  __syncthreads();
+  uint32_t total = 0;
+  if (lane == 0) {
+    for (uint32_t b = 0; b < kBins; ++b) {
+      const uint32_t c = w.cur[b];
+      w.cur[b] = total;
+      total += c;
+    }
+  }
+  total = __shfl_sync(0xFFFFFFFFu, total, 0);
+  __syncwarp();
 #pragma unroll
-  for (int j = 0; j < kPer; ++j)
-    if (bins[j] < kBins) order[off[bins[j]] + slot[j]] = req[j];
-  __syncthreads();
+  for (uint32_t j = 0; j < kLaneSlots; ++j) {
+    const uint32_t m = __match_any_sync(0xFFFFFFFFu, key[j]);
+    const uint32_t base = key[j] != kNone ? w.cur[key[j]] : 0u;
+    __syncwarp();
+    if (key[j] != kNone) {
+      if ((m & lt) == 0u) w.cur[key[j]] = base + __popc(m);
+      w.idx[base + __popc(m & lt)] = static_cast<uint16_t>(j * 32u + lane);
+    }
+    __syncwarp();
+  }
+  return total;
 }
+
+__device__ __forceinline__ uint32_t warp_global() {
+  return (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+}
+__device__ __forceinline__ uint32_t warps_total() { return (gridDim.x * blockDim.x) >> 5; }
 
 template <int V, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_alloc_batch(Ouroboros<V>* mm, const uint32_t* sizes, void** out,
                                                        uint32_t n) {
-  constexpr uint32_t T = BLOCK * kPer;
-  __shared__ uint32_t hist[kBins], off[kBins + 1];
-  __shared__ uint32_t order[T];
-  for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * T; t0 < n; t0 += static_cast<uint64_t>(gridDim.x) * T) {
-    uint32_t bins[kPer], req[kPer];
+  __shared__ WarpBins bins[BLOCK / 32];
+  WarpBins& w = bins[threadIdx.x >> 5];
+  const uint32_t lane = lane_id();
+  for (uint64_t t0 = static_cast<uint64_t>(warp_global()) * kWarpTile; t0 < n;
+       t0 += static_cast<uint64_t>(warps_total()) * kWarpTile) {
+    uint8_t key[kLaneSlots];
 #pragma unroll
-    for (int j = 0; j < kPer; ++j) {
-      const uint64_t i = t0 + static_cast<uint64_t>(j) * BLOCK + threadIdx.x;
-      req[j] = static_cast<uint32_t>(i);
-      bins[j] = i < n ? bin_of_size(sizes[i]) : kBins;
+    for (uint32_t j = 0; j < kLaneSlots; ++j) {
+      const uint64_t i = t0 + j * 32u + lane;
+      key[j] = static_cast<uint8_t>(i < n ? bin_of_size(sizes[i]) : kNone);
     }
-    bin_tile<BLOCK>(bins, req, hist, off, order);
-    const uint32_t cnt = off[kBins];
-    for (uint32_t k = threadIdx.x; k < cnt; k += BLOCK) {
-      const uint32_t i = order[k];
-      out[i] = mm->malloc(sizes[i]);
+    const uint32_t total = warp_bin(w, key);
+    for (uint32_t k = lane; k - lane < total; k += 32u) {
+      if (k < total) {
+        const uint64_t i = t0 + w.idx[k];
+        out[i] = mm->malloc(sizes[i]);
+      }
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
 template <int V, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_free_batch(Ouroboros<V>* mm, void* const* ptrs, uint32_t n) {
-  constexpr uint32_t T = BLOCK * kPer;
-  __shared__ uint32_t hist[kBins], off[kBins + 1];
-  __shared__ uint32_t order[T];
-  for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * T; t0 < n; t0 += static_cast<uint64_t>(gridDim.x) * T) {
-    uint32_t bins[kPer], req[kPer];
+  __shared__ WarpBins bins[BLOCK / 32];
+  WarpBins& w = bins[threadIdx.x >> 5];
+  const uint32_t lane = lane_id();
+  for (uint64_t t0 = static_cast<uint64_t>(warp_global()) * kWarpTile; t0 < n;
+       t0 += static_cast<uint64_t>(warps_total()) * kWarpTile) {
+    uint8_t key[kLaneSlots];
 #pragma unroll
-    for (int j = 0; j < kPer; ++j) {
-      const uint64_t i = t0 + static_cast<uint64_t>(j) * BLOCK + threadIdx.x;
-      req[j] = static_cast<uint32_t>(i);
-      bins[j] = i < n && ptrs[i] ? bin_of_ptr(mm, ptrs[i]) : kBins;
+    for (uint32_t j = 0; j < kLaneSlots; ++j) {
+      const uint64_t i = t0 + j * 32u + lane;
+      const void* p = i < n ? ptrs[i] : nullptr;
+      key[j] = static_cast<uint8_t>(p ? bin_of_ptr(mm, p) : kNone);
     }
-    bin_tile<BLOCK>(bins, req, hist, off, order);
-    const uint32_t cnt = off[kBins];
-    for (uint32_t k = threadIdx.x; k < cnt; k += BLOCK) mm->free(ptrs[order[k]]);
-    __syncthreads();
+    const uint32_t total = warp_bin(w, key);
+    for (uint32_t k = lane; k - lane < total; k += 32u)
+      if (k < total) mm->free(ptrs[t0 + w.idx[k]]);
+    __syncwarp();
   }
 }
 
@@ -141,49 +172,58 @@ __device__ __forceinline__ uint32_t draw_size(const SizeDist& d, uint64_t r) {
 
 // One cycle of churn over a live set: request i is picked with probability
 // fraction/1000 (hash of seed, cycle, i); a picked request frees its page and
-// allocates one of a freshly drawn size.  Frees of a tile go first (binned by
-// the class they release), then its allocations (binned by the new class).
+// allocates one of a freshly drawn size.  Per warp tile: the frees first,
+// sorted by the class they release, then the allocations, sorted by the new
+// class.
 template <int V, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_realloc_batch(Ouroboros<V>* mm, void** ptrs, uint32_t* sizes, uint32_t n,
                                                          uint64_t seed, uint32_t cycle, uint32_t fraction,
                                                          SizeDist dist) {
-  constexpr uint32_t T = BLOCK * kPer;
-  __shared__ uint32_t hist[kBins], off[kBins + 1];
-  __shared__ uint32_t order[T];
-  for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * T; t0 < n; t0 += static_cast<uint64_t>(gridDim.x) * T) {
-    uint32_t bins[kPer], req[kPer], news[kPer];
+  __shared__ WarpBins bins[BLOCK / 32];
+  WarpBins& w = bins[threadIdx.x >> 5];
+  const uint32_t lane = lane_id();
+  for (uint64_t t0 = static_cast<uint64_t>(warp_global()) * kWarpTile; t0 < n;
+       t0 += static_cast<uint64_t>(warps_total()) * kWarpTile) {
+    uint8_t key[kLaneSlots];
+    uint32_t picked = 0;   // bit j: slot j of this lane is picked
 #pragma unroll
-    for (int j = 0; j < kPer; ++j) {
-      const uint64_t i = t0 + static_cast<uint64_t>(j) * BLOCK + threadIdx.x;
-      req[j] = static_cast<uint32_t>(i);
-      bins[j] = kBins;
-      news[j] = 0;
+    for (uint32_t j = 0; j < kLaneSlots; ++j) {
+      const uint64_t i = t0 + j * 32u + lane;
+      key[j] = kNone;
       if (i < n) {
         const uint64_t r = mix64(seed ^ (static_cast<uint64_t>(cycle) << 32) ^ i);
         if ((r & 0x3FFu) < fraction * 1024u / 1000u) {
-          news[j] = draw_size(dist, mix64(r));
-          bins[j] = ptrs[i] ? bin_of_ptr(mm, ptrs[i]) : kBins;
-          if (!ptrs[i]) bins[j] = kBins + 1u;   // picked, nothing to free
+          picked |= 1u << j;
+          const void* p = ptrs[i];
+          if (p) key[j] = static_cast<uint8_t>(bin_of_ptr(mm, p));
         }
       }
     }
-    // frees (bins >= kBins are skipped by the binning)
-    bin_tile<BLOCK>(bins, req, hist, off, order);
-    for (uint32_t k = threadIdx.x; k < off[kBins]; k += BLOCK) mm->free(ptrs[order[k]]);
-    __syncthreads();
-    // allocations of the picked requests
+    uint32_t total = warp_bin(w, key);
+    for (uint32_t k = lane; k - lane < total; k += 32u)
+      if (k < total) mm->free(ptrs[t0 + w.idx[k]]);
+    __syncwarp();
+    // new sizes of the picked requests, then their allocations
 #pragma unroll
-    for (int j = 0; j < kPer; ++j) bins[j] = news[j] ? bin_of_size(news[j]) : kBins;
-    bin_tile<BLOCK>(bins, req, hist, off, order);
-#pragma unroll
-    for (int j = 0; j < kPer; ++j)
-      if (news[j]) sizes[req[j]] = news[j];
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < off[kBins]; k += BLOCK) {
-      const uint32_t i = order[k];
-      ptrs[i] = mm->malloc(sizes[i]);
+    for (uint32_t j = 0; j < kLaneSlots; ++j) {
+      key[j] = kNone;
+      if (picked & (1u << j)) {
+        const uint64_t i = t0 + j * 32u + lane;
+        const uint64_t r = mix64(seed ^ (static_cast<uint64_t>(cycle) << 32) ^ i);
+        const uint32_t sz = draw_size(dist, mix64(r));
+        sizes[i] = sz;
+        key[j] = static_cast<uint8_t>(bin_of_size(sz));
+      }
     }
-    __syncthreads();
+    __syncwarp();
+    total = warp_bin(w, key);
+    for (uint32_t k = lane; k - lane < total; k += 32u) {
+      if (k < total) {
+        const uint64_t i = t0 + w.idx[k];
+        ptrs[i] = mm->malloc(sizes[i]);
+      }
+    }
+    __syncwarp();
   }
 }
 
@@ -196,8 +236,8 @@ unsigned batch_grid(K kernel, int block, uint32_t n, int blocks_per_sm) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kernel, block, 0);
   if (fit < 1) fit = 1;
   if (blocks_per_sm > 0 && blocks_per_sm < fit) fit = blocks_per_sm;
-  const uint64_t tiles = (static_cast<uint64_t>(n) + static_cast<uint64_t>(block) * kPer - 1u) /
-                         (static_cast<uint64_t>(block) * kPer);
+  const uint64_t per_block = static_cast<uint64_t>(block / 32) * kWarpTile;
+  const uint64_t tiles = (static_cast<uint64_t>(n) + per_block - 1u) / per_block;
   const uint64_t g = static_cast<uint64_t>(sms) * fit;
   return static_cast<unsigned>(tiles < g ? (tiles ? tiles : 1u) : g);
 }
@@ -213,8 +253,6 @@ int with_block(int block, Launch&& launch) {
   switch (block) {
     case 128: return launch(std::integral_constant<int, 128>{});
     case 256: return launch(std::integral_constant<int, 256>{});
-    case 512: return launch(std::integral_constant<int, 512>{});
-    case 1024: return launch(std::integral_constant<int, 1024>{});
     default: return OURO_ERR_ARG;
   }
 }
@@ -310,8 +348,8 @@ int ouro_autotune_batch(ouro_heap* h, uint32_t n, uint32_t lo, uint32_t hi, int*
   cudaEventCreate(&e1);
   int best_b = 256, best_s = 0, rc = OURO_OK;
   float best_ms = 1e30f;
-  const int blocks[] = {128, 256, 512, 1024};
-  const int per_sm[] = {0, 1, 2, 4};
+  const int blocks[] = {128, 256};
+  const int per_sm[] = {0, 2, 4};
   for (int b : blocks) {
     for (int s : per_sm) {
       h->batch_block = b;

@@ -75,17 +75,16 @@ __device__ __forceinline__ void sem_mark_short(ClassState* q, uint32_t missing) 
   if (missing) atomicAdd(&q->holes, static_cast<int32_t>(missing));
 }
 
-// A waiting group hands back its demand of n pages: holes go down by as much
-// (not below zero; a CAS loop, out-of-memory path only).
+// A waiting group hands back its demand of n pages: holes go down by as much,
+// but not below zero.  One subtract, and the part that went below zero is
+// added back; whatever the interleaving, the net effect of each hand-back is
+// -max(holes it saw, 0) capped at n, so the count ends at max(holes - sum, 0)
+// and only dips below zero in between (a waiter that reads the dip polls
+// again).
 __device__ __forceinline__ void sem_hand_back(ClassState* q, uint32_t n) {
   atomicAdd(&q->sem.v, SemWord::give(n));
-  int32_t h = ld_relaxed(&q->holes);
-  for (uint32_t tries = 0; h > 0 && tries < 64u; ++tries) {
-    const int32_t nh = h > static_cast<int32_t>(n) ? h - static_cast<int32_t>(n) : 0;
-    const int32_t seen = atomicCAS(&q->holes, h, nh);
-    if (seen == h) break;
-    h = seen;
-  }
+  const int32_t old = atomicSub(&q->holes, static_cast<int32_t>(n));
+  if (old < static_cast<int32_t>(n)) atomicAdd(&q->holes, static_cast<int32_t>(n) - (old > 0 ? old : 0));
 }
 
 // BulkSemaphore_impl.cuh:7-17 tryReduce: take n pages only if all of them are

@@ -59,6 +59,9 @@ class Server:
     def __init__(self, graph: Graph, max_inflight: int = 64, watermark: float = 0.10, ring: int = 4096,
                  idle_seconds: float = 10.0, blocks_per_sm: int = 0):
         self.g = graph
+        # the loop occupies the device until it is stopped: pending work is
+        # finished first, and nothing while it runs may synchronize the device
+        torch.cuda.synchronize()
         cfg = ServeConfig(int(ring), int(max_inflight), int(blocks_per_sm), float(watermark), float(idle_seconds))
         h = ctypes.c_void_p()
         _check(lib().ouro_serve_start(graph.heap._handle(), _addr(graph.vptr), _addr(graph.degree), graph.nv,
@@ -117,8 +120,11 @@ class Server:
         """batches: list of (arrival_s, client, vertices tensor on the device),
         sorted by arrival (all at 0 for a saturating load).  Submits each at its
         arrival time, polls completions meanwhile, stops after the last one and
-        reports latencies from the device timestamps (seen -> done)."""
-        torch.cuda.synchronize()
+        reports latencies from the device timestamps (seen -> done).  The
+        batches' vertex tensors must be ready on the caller's stream; only that
+        stream is synchronized (a device-wide synchronize would wait for the
+        loop itself)."""
+        torch.cuda.current_stream().synchronize()
         requests = sum(int(b[2].numel()) for b in batches)
         t0 = time.perf_counter()
         full_waits = 0
