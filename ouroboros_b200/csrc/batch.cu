@@ -5,13 +5,17 @@
 // The per-thread path forms warp groups from whatever sizes a warp's 32
 // threads happen to ask for; with mixed sizes that is ~10 classes per warp,
 // so every class's semaphore and queue atomics are issued by groups of ~3
-// lanes.  Here every warp takes tiles of 1,024 requests (32 per lane),
+// lanes.  Here every warp takes tiles of 512 requests (16 per lane),
 // counting-sorts the tile by size class in its own part of shared memory (a
 // histogram and a scatter of request indices, match_any-ranked, no block
 // barrier), and serves it in sorted order: the 32 lanes of a round then ask
 // for one class (two at a class boundary), so a round costs one semaphore and
-// one queue reservation instead of ten.  Warps never wait for each other: a
-// warp whose tile holds the slow large classes does not hold up the others.
+// one queue reservation instead of ten.  Each warp starts its sorted order at
+// a different class (the class order is rotated by the warp's index), so the
+// warps of the grid spread over the classes' hot lines at every moment
+// instead of all serving the smallest class first.  Warps never wait for each
+// other: a warp whose tile holds the slow large classes does not hold up the
+// others.
 // Tiles are taken grid-stride by a persistent grid (no counter to reset, so
 // launches can be captured in CUDA graphs).  Frees are sorted by the class of
 // the page they release.
@@ -27,7 +31,7 @@ namespace {
 
 constexpr uint32_t kBins = kNumClasses + 1u;   // + the CUDA device heap
 constexpr uint32_t kNone = 15u;                // a slot without a request
-constexpr uint32_t kLaneSlots = 32u;           // requests per lane and tile
+constexpr uint32_t kLaneSlots = 16u;           // requests per lane and tile
 constexpr uint32_t kWarpTile = 32u * kLaneSlots;
 
 __device__ __forceinline__ uint32_t bin_of_size(uint64_t size) {
@@ -55,9 +59,10 @@ struct WarpBins {
 
 // Counting sort of the warp's tile slots by key (key[j] of this lane's slot
 // j, slot number j x 32 + lane; kNone: no request).  Writes the slot numbers
-// grouped by key into w.idx and returns how many there are.  Ranks come from
-// match_any, so the order within a key is the slot order.
-__device__ __forceinline__ uint32_t warp_bin(WarpBins& w, const uint8_t (&key)[kLaneSlots]) {
+// grouped by key into w.idx, bins in the order rot, rot + 1, ... (mod kBins),
+// and returns how many there are.  Ranks come from match_any, so the order
+// within a key is the slot order.
+__device__ __forceinline__ uint32_t warp_bin(WarpBins& w, const uint8_t (&key)[kLaneSlots], uint32_t rot) {
   const uint32_t lane = lane_id();
   const uint32_t lt = (1u << lane) - 1u;
   if (lane < 16u) w.cur[lane] = 0;
@@ -70,7 +75,8 @@ __device__ __forceinline__ uint32_t warp_bin(WarpBins& w, const uint8_t (&key)[k
   }
   uint32_t total = 0;
   if (lane == 0) {
-    for (uint32_t b = 0; b < kBins; ++b) {
+    for (uint32_t i = 0; i < kBins; ++i) {
+      const uint32_t b = (rot + i) % kBins;
       const uint32_t c = w.cur[b];
       w.cur[b] = total;
       total += c;
@@ -111,7 +117,7 @@ __global__ void __launch_bounds__(BLOCK) k_alloc_batch(Ouroboros<V>* mm, const u
       const uint64_t i = t0 + j * 32u + lane;
       key[j] = static_cast<uint8_t>(i < n ? bin_of_size(sizes[i]) : kNone);
     }
-    const uint32_t total = warp_bin(w, key);
+    const uint32_t total = warp_bin(w, key, warp_global() % kBins);
     for (uint32_t k = lane; k - lane < total; k += 32u) {
       if (k < total) {
         const uint64_t i = t0 + w.idx[k];
@@ -136,7 +142,7 @@ __global__ void __launch_bounds__(BLOCK) k_free_batch(Ouroboros<V>* mm, void* co
       const void* p = i < n ? ptrs[i] : nullptr;
       key[j] = static_cast<uint8_t>(p ? bin_of_ptr(mm, p) : kNone);
     }
-    const uint32_t total = warp_bin(w, key);
+    const uint32_t total = warp_bin(w, key, warp_global() % kBins);
     for (uint32_t k = lane; k - lane < total; k += 32u)
       if (k < total) mm->free(ptrs[t0 + w.idx[k]]);
     __syncwarp();
@@ -199,7 +205,7 @@ __global__ void __launch_bounds__(BLOCK) k_realloc_batch(Ouroboros<V>* mm, void*
         }
       }
     }
-    uint32_t total = warp_bin(w, key);
+    uint32_t total = warp_bin(w, key, warp_global() % kBins);
     for (uint32_t k = lane; k - lane < total; k += 32u)
       if (k < total) mm->free(ptrs[t0 + w.idx[k]]);
     __syncwarp();
@@ -216,7 +222,7 @@ __global__ void __launch_bounds__(BLOCK) k_realloc_batch(Ouroboros<V>* mm, void*
       }
     }
     __syncwarp();
-    total = warp_bin(w, key);
+    total = warp_bin(w, key, warp_global() % kBins);
     for (uint32_t k = lane; k - lane < total; k += 32u) {
       if (k < total) {
         const uint64_t i = t0 + w.idx[k];

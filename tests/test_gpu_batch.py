@@ -32,7 +32,7 @@ def _check_live(heap, ptrs, sizes, n, seed):
     assert rep["overlaps"] == 0 and rep["misaligned"] == 0 and rep["out_of_heap"] == 0, rep
 
 
-@pytest.mark.parametrize("block", [128, 1024])
+@pytest.mark.parametrize("block", [128, 256])
 @pytest.mark.parametrize("v", ob.VARIANTS)
 def test_batch_alloc_free_mixed_sizes(v, block):
     n = 1 << 18
