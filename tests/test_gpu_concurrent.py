@@ -126,8 +126,11 @@ def test_out_of_memory_virtualized(v, size):
             rep, nulls, bad = _round(heap, ptrs, n, size, seed=r)
             ok = n - nulls
             oks.append(ok)
-            # one group of 32 may find the budget momentarily full
-            assert cap - 32 * ppc <= ok <= cap, (r, ok, cap, mc)
+            # one group of 32 may find the budget momentarily full; the budget's
+            # queue-chunk term is computed on reserved page counts that may still
+            # hold releases in flight, so it can be one queue chunk short (the
+            # per-class margin absorbs that): at most one chunk's pages above cap
+            assert cap - 32 * ppc <= ok <= cap + ppc, (r, ok, cap, mc)
             assert bad == 0 and rep["overlaps"] == 0 and rep["misaligned"] == 0
             _idle(heap, v)
         assert oks[1] == oks[2], oks
