@@ -741,6 +741,7 @@ def batched_bench(n: int, cycles: int, stream) -> dict:
             heap.alloc_batch(sizes, ptrs, n, stream=stream)
         stream.synchronize()
         sizes_live = sizes.clone()
+        heap.batch_reserve(n)   # the batch scratch exists before capture (no allocation inside the graph)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=stream):
             for c in range(cycles):

@@ -219,14 +219,19 @@ int ouro_allocate_chunk(ouro_heap* h, uint32_t* out_chunk);
 int ouro_enqueue_initial_chunk(ouro_heap* h, uint32_t queue_index, uint32_t chunk_index, uint32_t available_pages);
 
 /* The batched path (no counterpart in the reference, whose only caller is its
- * per-thread benchmark): persistent kernels serve n requests in warp tiles of
- * 1,024; each warp counting-sorts its tile by size class in its own part of
- * shared memory and serves it in sorted order, so the lanes of a round ask for
- * the same class and a round of 32 requests costs one semaphore and one queue
- * reservation; warps never wait for one another.  block = 0 takes the shape
- * ouro_autotune_batch picked (256 until then); else 128 or 256.
- * Stream-ordered; the kernels keep no state between launches and can be
- * captured in a CUDA graph.
+ * per-thread benchmark): a batch is counting-sorted by size class on the
+ * device (per-tile histograms in shared memory, a scan, a scatter of request
+ * indices) and then served by one launch with a thread per request in sorted
+ * order, so every warp but the one at each class boundary asks for one class
+ * with all 32 lanes.  Frees are sorted by the class of the page they release.
+ * block (of the serving launch) = 0 takes the size ouro_autotune_batch picked
+ * (256 until then); else 128, 256, 512 or 1024.  Stream-ordered; the sort
+ * uses the heap's batch scratch (4 bytes per request plus 64 per 4,096),
+ * which a call for more requests than before allocates (cudaMalloc, so not
+ * during stream capture: call ouro_batch_reserve first).  A reserved batch
+ * cycle can be captured in a CUDA graph and replayed; calls on one heap
+ * share the scratch, so concurrent batch calls on one heap must be ordered.
+ *   ouro_batch_reserve: scratch for batches of up to n requests.
  *   ouro_alloc_batch:   d_out[i] = malloc(d_sizes[i])
  *   ouro_free_batch:    free(d_ptrs[i]) (nullptr skipped)
  *   ouro_realloc_batch: one churn cycle over a live set: request i is picked
@@ -239,15 +244,17 @@ typedef struct {
   uint32_t lo, hi;
   float zipf_s;
 } ouro_size_dist;
+int ouro_batch_reserve(ouro_heap* h, uint32_t n);
 int ouro_alloc_batch(ouro_heap* h, const uint32_t* d_sizes, void** d_out, uint32_t n, int block, void* stream);
 int ouro_free_batch(ouro_heap* h, void* const* d_ptrs, uint32_t n, int block, void* stream);
 int ouro_realloc_batch(ouro_heap* h, void** d_ptrs, uint32_t* d_sizes, uint32_t n, uint64_t seed, uint32_t cycle,
                        uint32_t fraction_permille, const ouro_size_dist* dist, int block, void* stream);
 /* Autotuner of the batched path: times alloc + free batches of n log-uniform
- * sizes in [lo, hi] on this heap for both block sizes (128, 256) and
- * resident blocks per SM (all that fit, 2, 4), keeps the fastest as the
- * heap's batched launch shape and reports it (Mops/s counts mallocs + frees).
- * Uses the heap: call it on an idle heap.  Allocates scratch; synchronous. */
+ * sizes in [lo, hi] on this heap for every block size of the serving launch
+ * (128 .. 1024), keeps the fastest as the heap's batched launch shape and
+ * reports it (Mops/s counts mallocs + frees; *out_per_sm is 0: the serving
+ * launch is not persistent).  Uses the heap: call it on an idle heap.
+ * Allocates scratch; synchronous. */
 int ouro_autotune_batch(ouro_heap* h, uint32_t n, uint32_t lo, uint32_t hi, int* out_block, int* out_per_sm,
                         double* out_mops);
 

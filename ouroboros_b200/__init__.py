@@ -41,7 +41,7 @@ EXPORTS = (
     "ouro_status_string", "ouro_check_allocations_noalloc", "ouro_free_resources", "ouro_prefill",
     "ouro_alloc_batch", "ouro_free_batch", "ouro_realloc_batch", "ouro_autotune_batch",
     "ouro_graph_init", "ouro_graph_grow", "ouro_graph_check", "ouro_free_bytes_to",
-    "ouro_allocate_chunk", "ouro_enqueue_initial_chunk",
+    "ouro_allocate_chunk", "ouro_enqueue_initial_chunk", "ouro_batch_reserve",
     "ouro_serve_start", "ouro_serve_submit", "ouro_serve_poll", "ouro_serve_stop", "ouro_serve_close",
 )
 
@@ -138,6 +138,7 @@ def lib():
         L.ouro_serve_close.argtypes = [p]
         L.ouro_enqueue_initial_chunk.argtypes = [p, u32, u32, u32]
         L.ouro_alloc_batch.argtypes = [p, p, p, u32, i, p]
+        L.ouro_batch_reserve.argtypes = [p, u32]
         L.ouro_free_batch.argtypes = [p, p, u32, i, p]
         L.ouro_realloc_batch.argtypes = [p, p, p, u32, u64, u32, u32, ctypes.POINTER(_SizeDist), i, p]
         L.ouro_graph_init.argtypes = [p, p, p, p, u32, u64, ctypes.c_float, p, p]
@@ -280,6 +281,10 @@ class Ouroboros:
         return {k: int(x) for k, x in zip(names, out)}
 
     # -- batched path ---------------------------------------------------------
+    def batch_reserve(self, n: int):
+        """Scratch for batches of up to n requests (call before capturing batch calls in a graph)."""
+        _check(lib().ouro_batch_reserve(self._handle(), n), "ouro_batch_reserve")
+
     def alloc_batch(self, sizes, out_ptrs, n: int, block: int = 0, stream=None):
         """out_ptrs[i] = malloc(sizes[i]), binned by size class per tile."""
         _check(lib().ouro_alloc_batch(self._handle(), _addr(sizes), _addr(out_ptrs), n, block, _stream(stream)),

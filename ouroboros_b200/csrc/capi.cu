@@ -386,6 +386,7 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
 
 int ouro_destroy(ouro_heap* h) {
   if (!h) return OURO_ERR_ARG;
+  if (h->batch_scratch) cudaFree(h->batch_scratch);
   cudaError_t e = cudaFree(h->raw);
   delete h;
   return cuda_rc(e);

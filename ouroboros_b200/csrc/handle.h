@@ -17,8 +17,10 @@ struct ouro_heap {
   void* raw;
   ouro::HeapCore* dev;
   char* base;
-  int batch_block;    // batched path launch shape picked by ouro_autotune_batch (0: default)
-  int batch_per_sm;   // resident blocks per SM for it (0: as many as fit)
+  int batch_block;    // batched path: block size of the serving launch picked by ouro_autotune_batch (0: default)
+  int batch_per_sm;   // kept for the C ABI's report; the serving launch is not persistent
+  void* batch_scratch;              // batched path: sort counters and permutation (grown on demand)
+  size_t batch_scratch_bytes;
 };
 
 namespace ouro {
