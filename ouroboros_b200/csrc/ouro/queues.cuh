@@ -121,8 +121,10 @@ __device__ uint32_t page_grow(HeapCore* h, ClassState* q, const Group& g, uint32
     __threadfence();
   }
   if (g.is_leader()) {
-    if (owed && got < k) sem_mark_short(q, (k - got) * q->ppc);
+    // the pages first, then the holes: a group that resolves on seeing the
+    // holes already counts the pages that did arrive
     sem_signal(q, E);
+    if (owed && got < k) sem_mark_short(q, (k - got) * q->ppc);
   }
   return got;
 }
@@ -366,8 +368,8 @@ __device__ uint32_t chunk_grow(HeapCore* h, ClassState* q, const Group& g, uint3
   __syncwarp(g.mask);
   __threadfence();
   if (g.is_leader()) {
+    sem_signal(q, got * q->ppc);   // pages first, then holes (as in page_grow)
     if (owed && got < k) sem_mark_short(q, (k - got) * q->ppc);
-    sem_signal(q, got * q->ppc);
   }
   return got;
 }

@@ -105,10 +105,12 @@ __device__ __forceinline__ bool sem_try_reduce(ClassState* q, uint32_t n) {
 // Take up to n pages that are there with fetch-adds only.  A group that took
 // more than was there hands the excess back; if the count is positive after
 // its hand-back (other groups' excess was in flight) and it still needs
-// pages, it tries again.  Returns the pages taken.
+// pages, it tries again after a short pause, so that many resolving groups do
+// not keep the count oscillating.  Returns the pages taken.
 __device__ inline uint32_t sem_take_upto(HeapCore* h, ClassState* q, uint32_t n) {
   uint32_t got = 0;
-  for (uint32_t round = 0; got < n && round < 256u; ++round) {
+  for (uint32_t round = 0, it = 0; got < n && round < 4096u; ++round) {
+    if (round) backoff(it);
     const uint32_t want = n - got;
     const unsigned long long old = atomicAdd(&q->sem.v, SemWord::take(want));
     const long long c0 = SemWord::count(old);
