@@ -59,6 +59,42 @@ typedef struct ouro_heap ouro_heap;
  * is the reference's for the same size.  Synchronous. */
 int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out);
 
+/* Run-time allocator parameters.  The reference fixes all of them at compile
+ * time (include/Parameters.h:9-18); ouro_config_default fills in its values,
+ * and ouro_create is ouro_create_config with them.
+ *   chunk_bytes            CHUNK_SIZE (Parameters.h:17, 16 B << 9 = 8192).  Only
+ *                          8192 is accepted: the 9 page bits of a queue entry
+ *                          (MemoryIndex.cuh:6-51) and the 512-bit occupancy
+ *                          mask of a chunk are sized for 8 KiB / 16 B.
+ *   page_queue_entries     page_queue_size (Parameters.h:11, 2^23): ring entries
+ *                          per size class of the standard queues (P, C); a power
+ *                          of two in [2^16, 2^23].
+ *   virtual_queue_entries  virtual_queue_size (Parameters.h:12, 16384): entries of
+ *                          the per-class index of queue chunks of the virtualized-
+ *                          array queues (VAP, VAC), each queue chunk holding 2048
+ *                          queue entries; a power of two in [32, 16384].
+ *   agg_width              lanes whose requests of one size class are aggregated
+ *                          into one group (one semaphore and one queue atomic per
+ *                          group): 1, 2, 4, 8, 16 or 32.  The reference
+ *                          aggregates over the whole warp (__match_any_sync over
+ *                          __activemask(), BulkSemaphore_impl.cuh:124-127): 32.
+ * The number of usable chunks follows the reference's capacity formula
+ * (MemoryInitialization.cuh:156-166) on the configured queue sizes, so with
+ * the defaults it is the reference's.  The linked-list variants have no queue
+ * arrays; the two queue sizes do not apply to them. */
+typedef struct {
+  uint32_t chunk_bytes;
+  uint32_t page_queue_entries;
+  uint32_t virtual_queue_entries;
+  uint32_t agg_width;
+} ouro_config;
+
+int ouro_config_default(ouro_config* out);
+/* ouro_create with explicit parameters (cfg NULL = the defaults). */
+int ouro_create_config(int variant, uint64_t heap_bytes, const ouro_config* cfg, ouro_heap** out);
+/* The parameters a heap was created with. */
+int ouro_get_config(const ouro_heap* h, ouro_config* out);
+
 /* Memory::~Memory  (include/device/Ouroboros.cuh:11-15): frees the heap. */
 int ouro_destroy(ouro_heap* h);
 
@@ -257,6 +293,32 @@ int ouro_realloc_batch(ouro_heap* h, void** d_ptrs, uint32_t* d_sizes, uint32_t 
  * Allocates scratch; synchronous. */
 int ouro_autotune_batch(ouro_heap* h, uint32_t n, uint32_t lo, uint32_t hi, int* out_block, int* out_per_sm,
                         double* out_mops);
+/* Autotuner over the run-time configuration and the launch shape (no
+ * counterpart in the reference, whose parameters are compile-time,
+ * include/Parameters.h:9-18).  Every candidate gets a fresh heap of
+ * `variant` and `heap_bytes`, on which n requests with seeded log-uniform
+ * sizes in [lo, hi] are allocated and freed through the batched path: one
+ * untimed repetition, then `reps` timed ones (alloc + free, event-timed).
+ * Candidates: the queue capacities queue_entries[0..n_queue) (queue entries per
+ * size class: a standard ring of that many entries, a virtualized-array index
+ * of that many / 2048 queue chunks; not swept for the linked-list variants),
+ * the aggregation widths agg_widths[0..n_agg) and the block sizes of the
+ * serving launch blocks[0..n_blocks).  A candidate that returns a nullptr or
+ * raises an error flag is rejected (ok = 0).  points, if not NULL, receives
+ * every candidate (n_queue x n_agg x n_blocks entries, in that nesting
+ * order); *best the fastest accepted one (Mops/s counts mallocs + frees).
+ * OURO_ERR_DEVICE when no candidate is accepted.  Allocates its heaps and
+ * buffers; synchronous. */
+typedef struct {
+  ouro_config cfg;
+  int block;
+  int ok;
+  double mops;
+} ouro_tune_point;
+int ouro_autotune_config(int variant, uint64_t heap_bytes, uint32_t n, uint32_t lo, uint32_t hi, uint32_t reps,
+                         const uint32_t* queue_entries, uint32_t n_queue, const uint32_t* agg_widths,
+                         uint32_t n_agg, const int* blocks, uint32_t n_blocks, ouro_tune_point* points,
+                         ouro_tune_point* best);
 
 /* The dynamic-graph workload of the serving loop (no counterpart in the
  * reference; its consumer, ouroGraph, lives outside the reference tree).  A

@@ -140,6 +140,7 @@ def _rlib():
         lib.ref_alloc.argtypes = [p, u32, u32, p, p, i, p]
         lib.ref_free.argtypes = [p, u32, p, i, p]
         lib.ref_write.argtypes = [p, u32, u32, p, u32, p]
+        lib.ref_sanitize.argtypes = [p, p, u32, u32, p, p, p]
         lib.ref_verify.argtypes = [p, u32, u32, p, u32, p, p]
         lib.ref_run_cell.argtypes = [p, u32, u32, i, i, p, u32, p, p]
         _ref_lib = lib
@@ -204,6 +205,13 @@ class RefDriver:
         rc = self._lib.ref_free(self._h, n, d_ptrs, block, stream or None)
         if rc:
             raise OracleError(f"ref_free failed ({rc})")
+
+    def sanitize(self, n, size, d_ptrs, d_counters, d_sizes=0, stream=0):
+        """Null (and count in d_counters[1]) every pointer the reference returned
+        outside its chunk region, before anything writes through or frees it."""
+        rc = self._lib.ref_sanitize(self._h, d_ptrs, n, size, d_sizes or None, d_counters, stream or None)
+        if rc:
+            raise OracleError(f"ref_sanitize failed ({rc})")
 
     def run_cell(self, n, size, reps, d_ptrs, d_counters, seed=0x9E3779B9, block=256):
         ms = np.zeros(2, dtype=np.float32)

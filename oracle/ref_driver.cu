@@ -119,8 +119,30 @@ __global__ void k_verify(void** ptrs, uint32_t n, uint32_t size, const uint32_t*
   if (bad) atomicAdd(&counters[1], (unsigned long long)bad);
 }
 
+// The harness writes through, and the reference frees, the pointers the
+// reference's malloc returned.  A pointer outside the reference's chunk
+// region [d_data, d_data + maxChunks * 8320) -- which its code has no business
+// returning for requests of at most 8 KiB -- is replaced by nullptr here and
+// counted in counters[1], so that neither the pattern kernels nor the
+// reference's own free ever dereference it.
+__global__ void k_sanitize(void** ptrs, uint32_t n, uint32_t size, const uint32_t* sizes, const char* lo,
+                           const char* hi, unsigned long long* counters) {
+  uint32_t tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid >= n) return;
+  const char* p = reinterpret_cast<const char*>(ptrs[tid]);
+  if (!p) return;
+  const uint32_t sz = sizes ? sizes[tid] : size;
+  if (sz > 8192u) return;   // served by the CUDA device heap
+  if (p < lo || p + sz > hi) {
+    ptrs[tid] = nullptr;
+    atomicAdd(&counters[1], 1ull);
+  }
+}
+
 struct RefBase {
   virtual ~RefBase() {}
+  virtual int sanitize(void** ptrs, uint32_t n, uint32_t size, const uint32_t* sizes, unsigned long long* counters,
+                       cudaStream_t s) = 0;
   virtual int trace(const uint32_t* ops, uint64_t n, int64_t* off, uint32_t tid, uint32_t bid) = 0;
   virtual int state(uint64_t* out) = 0;
   virtual int alloc(uint32_t n, uint32_t size, const uint32_t* sizes, void** ptrs, int block, cudaStream_t s) = 0;
@@ -227,6 +249,15 @@ struct RefHeap : RefBase {
     return cudaGetLastError() == cudaSuccess ? 0 : 4;
   }
 
+  int sanitize(void** ptrs, uint32_t n, uint32_t size, const uint32_t* sizes, unsigned long long* counters,
+               cudaStream_t s) override {
+    if (n == 0) return 0;
+    const char* lo = reinterpret_cast<const char*>(mm.memory.d_data);
+    const char* hi = lo + static_cast<size_t>(mm.memory.maxChunks) * 8320u;
+    k_sanitize<<<(n + 255) / 256, 256, 0, s>>>(ptrs, n, size, sizes, lo, hi, counters);
+    return cudaGetLastError() == cudaSuccess ? 0 : 4;
+  }
+
   void info(uint64_t* out) override {
     out[0] = mm.memory.maxChunks;
     out[1] = mm.memory.allocationSize;
@@ -294,6 +325,12 @@ int ref_free(void* h, uint32_t n, void** d_ptrs, int block, void* stream) {
   return static_cast<RefBase*>(h)->free_(n, d_ptrs, block, static_cast<cudaStream_t>(stream));
 }
 
+int ref_sanitize(void* h, void** d_ptrs, uint32_t n, uint32_t size, const uint32_t* d_sizes,
+                 unsigned long long* d_counters, void* stream) {
+  if (!h || !d_ptrs || !d_counters) return 1;
+  return static_cast<RefBase*>(h)->sanitize(d_ptrs, n, size, d_sizes, d_counters, static_cast<cudaStream_t>(stream));
+}
+
 int ref_write(void** d_ptrs, uint32_t n, uint32_t size, const uint32_t* d_sizes, uint32_t seed, void* stream) {
   if (n == 0) return 0;
   k_write<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(d_ptrs, n, size, d_sizes, seed);
@@ -327,6 +364,7 @@ int ref_run_cell(void* h, uint32_t n, uint32_t size, int block, int reps, void**
     cudaEventSynchronize(b);
     cudaEventElapsedTime(&t, a, b);
     ms[0] += t;
+    rc |= r->sanitize(d_ptrs, n, size, nullptr, d_counters, 0);
     rc |= ref_write(d_ptrs, n, size, nullptr, seed + static_cast<uint32_t>(i), nullptr);
     rc |= ref_verify(d_ptrs, n, size, nullptr, seed + static_cast<uint32_t>(i), d_counters, nullptr);
     if (cudaDeviceSynchronize() != cudaSuccess) rc = 4;

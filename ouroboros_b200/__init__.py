@@ -43,6 +43,7 @@ EXPORTS = (
     "ouro_graph_init", "ouro_graph_grow", "ouro_graph_check", "ouro_free_bytes_to",
     "ouro_allocate_chunk", "ouro_enqueue_initial_chunk", "ouro_batch_reserve",
     "ouro_serve_start", "ouro_serve_submit", "ouro_serve_poll", "ouro_serve_stop", "ouro_serve_close",
+    "ouro_config_default", "ouro_create_config", "ouro_get_config", "ouro_autotune_config",
 )
 
 
@@ -53,6 +54,50 @@ class OuroError(RuntimeError):
 class _Info(ctypes.Structure):
     _fields_ = [("variant", ctypes.c_int32), ("heap_bytes", ctypes.c_uint64), ("max_chunks", ctypes.c_uint64),
                 ("alloc_bytes", ctypes.c_uint64), ("data_base", ctypes.c_uint64), ("data_end", ctypes.c_uint64)]
+
+
+class Config(ctypes.Structure):
+    """ouro_config: run-time parameters of a heap (defaults: the reference's
+    compile-time ones, include/Parameters.h:9-18)."""
+    _fields_ = [("chunk_bytes", ctypes.c_uint32), ("page_queue_entries", ctypes.c_uint32),
+                ("virtual_queue_entries", ctypes.c_uint32), ("agg_width", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+class TunePoint(ctypes.Structure):
+    _fields_ = [("cfg", Config), ("block", ctypes.c_int), ("ok", ctypes.c_int), ("mops", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {**self.cfg.as_dict(), "block": int(self.block), "ok": bool(self.ok), "mops": float(self.mops)}
+
+
+def autotune_config(variant: str, heap_bytes: int, n: int, lo: int = 16, hi: int = 8192, reps: int = 2,
+                    queue_entries=(1 << 16, 1 << 17, 1 << 18, 1 << 19, 1 << 20), agg_widths=(8, 16, 32),
+                    blocks=(128, 256, 512, 1024)) -> dict:
+    """ouro_autotune_config: every (queue capacity, aggregation width, block
+    size) candidate on a fresh heap, batched alloc + free of n log-uniform
+    sizes; returns {"best": ..., "points": [...]}."""
+    q = np.asarray(queue_entries, dtype=np.uint32)
+    a = np.asarray(agg_widths, dtype=np.uint32)
+    b = np.asarray(blocks, dtype=np.int32)
+    pts = (TunePoint * (len(q) * len(a) * len(b)))()
+    best = TunePoint()
+    _check(lib().ouro_autotune_config(VARIANTS.index(variant), int(heap_bytes), n, lo, hi, reps,
+                                      q.ctypes.data, len(q), a.ctypes.data, len(a), b.ctypes.data, len(b),
+                                      pts, ctypes.byref(best)), "ouro_autotune_config")
+    return {"best": best.as_dict(), "points": [p.as_dict() for p in pts]}
+
+
+def default_config(**overrides) -> Config:
+    c = Config()
+    _check(lib().ouro_config_default(ctypes.byref(c)), "ouro_config_default")
+    for k, v in overrides.items():
+        if not hasattr(c, k):
+            raise ValueError(f"unknown config field {k}")
+        setattr(c, k, int(v))
+    return c
 
 
 class _Status(ctypes.Structure):
@@ -112,6 +157,11 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         p, u32, u64, i = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
         L.ouro_create.argtypes = [i, u64, ctypes.POINTER(p)]
+        L.ouro_config_default.argtypes = [ctypes.POINTER(Config)]
+        L.ouro_create_config.argtypes = [i, u64, ctypes.POINTER(Config), ctypes.POINTER(p)]
+        L.ouro_get_config.argtypes = [p, ctypes.POINTER(Config)]
+        L.ouro_autotune_config.argtypes = [i, u64, u32, u32, u32, u32, p, u32, p, u32, p, u32,
+                                           ctypes.POINTER(TunePoint), ctypes.POINTER(TunePoint)]
         L.ouro_destroy.argtypes = [p]
         L.ouro_device_handle.argtypes = [p]
         L.ouro_device_handle.restype = p
@@ -178,11 +228,12 @@ def _stream(s) -> int | None:
 class Ouroboros:
     """One heap of one instantiation on the current device."""
 
-    def __init__(self, variant: str = "P", heap_bytes: int | None = None):
+    def __init__(self, variant: str = "P", heap_bytes: int | None = None, config: Config | dict | None = None):
         if variant not in VARIANTS:
             raise ValueError(f"variant must be one of {VARIANTS}")
         self.variant = variant
         self._h = None
+        self._config = default_config(**config) if isinstance(config, dict) else config
         if heap_bytes is not None:
             self.initialize(heap_bytes)
 
@@ -192,9 +243,18 @@ class Ouroboros:
         if self._h is not None:
             return self
         h = ctypes.c_void_p()
-        _check(lib().ouro_create(VARIANTS.index(self.variant), int(heap_bytes), ctypes.byref(h)), "ouro_create")
+        if self._config is None:
+            _check(lib().ouro_create(VARIANTS.index(self.variant), int(heap_bytes), ctypes.byref(h)), "ouro_create")
+        else:
+            _check(lib().ouro_create_config(VARIANTS.index(self.variant), int(heap_bytes), ctypes.byref(self._config),
+                                            ctypes.byref(h)), "ouro_create_config")
         self._h = h
         return self
+
+    def config(self) -> dict:
+        c = Config()
+        _check(lib().ouro_get_config(self._handle(), ctypes.byref(c)), "ouro_get_config")
+        return c.as_dict()
 
     def getDeviceMemoryManager(self) -> int:  # noqa: N802 (reference name)
         return int(lib().ouro_device_handle(self._handle()))

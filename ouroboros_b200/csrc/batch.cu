@@ -416,4 +416,80 @@ int ouro_autotune_batch(ouro_heap* h, uint32_t n, uint32_t lo, uint32_t hi, int*
   return rc;
 }
 
+int ouro_autotune_config(int variant, uint64_t heap_bytes, uint32_t n, uint32_t lo, uint32_t hi, uint32_t reps,
+                         const uint32_t* queue_entries, uint32_t n_queue, const uint32_t* agg_widths,
+                         uint32_t n_agg, const int* blocks, uint32_t n_blocks, ouro_tune_point* points,
+                         ouro_tune_point* best) {
+  if (variant < 0 || variant > 5 || n == 0 || lo < 1u || hi < lo || reps == 0 || !queue_entries || n_queue == 0 ||
+      !agg_widths || n_agg == 0 || !blocks || n_blocks == 0 || !best)
+    return OURO_ERR_ARG;
+  for (uint32_t b = 0; b < n_blocks; ++b)
+    if (blocks[b] != 128 && blocks[b] != 256 && blocks[b] != 512 && blocks[b] != 1024) return OURO_ERR_ARG;
+  void** ptrs = nullptr;
+  uint32_t* sizes = nullptr;
+  if (cudaMalloc(&ptrs, static_cast<size_t>(n) * sizeof(void*)) != cudaSuccess ||
+      cudaMalloc(&sizes, static_cast<size_t>(n) * sizeof(uint32_t)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    cudaFree(ptrs);
+    return OURO_ERR_NOMEM;
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const ouro_size_dist dist{0, lo, hi, 0.0f};
+  const bool linked = variant / 2 == 2;
+  int rc = OURO_OK;
+  best->ok = 0;
+  best->mops = 0.0;
+  for (uint32_t qi = 0; qi < n_queue && rc == OURO_OK; ++qi) {
+    for (uint32_t ai = 0; ai < n_agg && rc == OURO_OK; ++ai) {
+      ouro_config cfg;
+      ouro_config_default(&cfg);
+      if (variant / 2 == 0) cfg.page_queue_entries = queue_entries[qi];
+      if (variant / 2 == 1) cfg.virtual_queue_entries = queue_entries[qi] / kQcSpots;
+      cfg.agg_width = agg_widths[ai];
+      ouro_heap* h = nullptr;
+      // the linked-list variants have no queue arrays: one queue candidate
+      const bool skip = linked && qi > 0;
+      const int crc = skip ? OURO_ERR_ARG : ouro_create_config(variant, heap_bytes, &cfg, &h);
+      if (crc == OURO_ERR_CUDA || crc == OURO_ERR_NOMEM) rc = crc;
+      for (uint32_t bi = 0; bi < n_blocks; ++bi) {
+        ouro_tune_point pt{cfg, blocks[bi], 0, 0.0};
+        if (h && rc == OURO_OK) {
+          cudaMemset(ptrs, 0, static_cast<size_t>(n) * sizeof(void*));
+          // the sizes: one churn cycle that picks every request draws them
+          // (and allocates them, which is the untimed repetition)
+          int r = ouro_realloc_batch(h, ptrs, sizes, n, 0x5EEDull, 0u, 1000u, &dist, blocks[bi], nullptr);
+          if (r == OURO_OK) r = ouro_free_batch(h, ptrs, n, blocks[bi], nullptr);
+          float ms_total = 0.f;
+          for (uint32_t rep = 0; rep < reps && r == OURO_OK; ++rep) {
+            cudaEventRecord(e0);
+            r = ouro_alloc_batch(h, sizes, ptrs, n, blocks[bi], nullptr);
+            if (r == OURO_OK) r = ouro_free_batch(h, ptrs, n, blocks[bi], nullptr);
+            cudaEventRecord(e1);
+            if (r == OURO_OK && cudaEventSynchronize(e1) != cudaSuccess) r = OURO_ERR_CUDA;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms_total += ms;
+          }
+          ouro_heap_status st{};
+          if (r == OURO_OK) r = ouro_get_status(h, &st, 0);
+          if (r == OURO_ERR_CUDA) rc = r;
+          pt.ok = r == OURO_OK && st.flags == 0u && st.null_results == 0u && ms_total > 0.f;
+          pt.mops = ms_total > 0.f ? 2.0 * n * reps / (ms_total * 1e-3) / 1e6 : 0.0;
+        }
+        if (points) points[(qi * n_agg + ai) * n_blocks + bi] = pt;
+        if (pt.ok && pt.mops > best->mops) *best = pt;
+      }
+      if (h) ouro_destroy(h);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(ptrs);
+  cudaFree(sizes);
+  if (rc == OURO_OK && !best->ok) rc = OURO_ERR_DEVICE;
+  return rc;
+}
+
 }  // extern "C"

@@ -281,11 +281,39 @@ const char* ouro_status_string(int code) {
   }
 }
 
+int ouro_config_default(ouro_config* out) {
+  if (!out) return OURO_ERR_ARG;
+  out->chunk_bytes = kChunkBytes;
+  out->page_queue_entries = kRingSize;
+  out->virtual_queue_entries = kVqSize;
+  out->agg_width = 32u;
+  return OURO_OK;
+}
+
 int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
+  return ouro_create_config(variant, heap_bytes, nullptr, out);
+}
+
+int ouro_get_config(const ouro_heap* h, ouro_config* out) {
+  if (!h || !out) return OURO_ERR_ARG;
+  *out = h->cfg;
+  return OURO_OK;
+}
+
+int ouro_create_config(int variant, uint64_t heap_bytes, const ouro_config* cfg_in, ouro_heap** out) {
   if (!out || variant < 0 || variant > 5) return OURO_ERR_ARG;
   *out = nullptr;
+  ouro_config cfg;
+  ouro_config_default(&cfg);
+  if (cfg_in) cfg = *cfg_in;
+  auto pow2 = [](uint32_t v) { return v && (v & (v - 1u)) == 0u; };
+  if (cfg.chunk_bytes != kChunkBytes || !pow2(cfg.page_queue_entries) || cfg.page_queue_entries < (1u << 16) ||
+      cfg.page_queue_entries > kRingSize || !pow2(cfg.virtual_queue_entries) || cfg.virtual_queue_entries < 32u ||
+      cfg.virtual_queue_entries > kVqSize || !pow2(cfg.agg_width) || cfg.agg_width > 32u)
+    return OURO_ERR_ARG;
   Layout L;
-  if (!compute_layout(variant / 2, heap_bytes, &L)) return OURO_ERR_ARG;
+  if (!compute_layout(variant / 2, heap_bytes, &L, cfg.page_queue_entries, cfg.virtual_queue_entries))
+    return OURO_ERR_ARG;
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) return OURO_ERR_CUDA;
   {
@@ -307,6 +335,7 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
   h->variant = variant;
   h->heap_bytes = heap_bytes;
   h->L = L;
+  h->cfg = cfg;
   h->device = device;
   if (cudaMalloc(&h->raw, L.alloc_bytes) != cudaSuccess) {
     (void)cudaGetLastError();
@@ -321,7 +350,9 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
   if (e == cudaSuccess) e = cudaMemset(h->base + L.data_off, 0xFF, L.ring_off - L.data_off);
   const unsigned long long q_end = L.reuse_off + 2ull * kReuseSize * 4u;
   if (e == cudaSuccess) e = cudaMemset(h->base + L.ring_off, 0xFF, q_end - L.ring_off);
-  if (e == cudaSuccess && variant / 2 == 0) e = cudaMemset(h->base + L.seg_off, 0, kNumClasses * kRingSegs * 4ull);
+  const uint32_t ring = static_cast<uint32_t>(L.ring_entries), vq = static_cast<uint32_t>(L.vq_entries);
+  const uint32_t segs = ring / kQcSpots;
+  if (e == cudaSuccess && variant / 2 == 0) e = cudaMemset(h->base + L.seg_off, 0, kNumClasses * segs * 4ull);
   HeapCore core;
   std::memset(&core, 0, sizeof(core));
   core.variant = variant;
@@ -332,6 +363,7 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
   core.base = h->base;
   core.alloc_bytes = L.alloc_bytes;
   core.heap_bytes = heap_bytes;
+  core.agg_width = cfg.agg_width;
   const int kind = variant / 2;
   if (kind != 0) {
     // usable base chunks (index + 1 < max_chunks); every class starts with
@@ -352,14 +384,15 @@ int ouro_create(int variant, uint64_t heap_bytes, ouro_heap** out) {
     q.front_ptr = q.back_ptr = q.old_ptr = kEmpty;
     q.clean_on_recycle = (variant % 2) == 1 ? 1u : 0u;
     if (kind == 0) {
-      q.ring = reinterpret_cast<uint32_t*>(h->base + L.ring_off) + static_cast<size_t>(c) * kRingSize;
-      q.ring_mask = kRingSize - 1u;
-      q.page_cap = kRingSize;
-      q.seg = reinterpret_cast<uint32_t*>(h->base + L.seg_off) + static_cast<size_t>(c) * kRingSegs;
+      q.ring = reinterpret_cast<uint32_t*>(h->base + L.ring_off) + static_cast<size_t>(c) * ring;
+      q.ring_mask = ring - 1u;
+      q.page_cap = ring;
+      q.seg = reinterpret_cast<uint32_t*>(h->base + L.seg_off) + static_cast<size_t>(c) * segs;
+      q.seg_mask = segs - 1u;
     } else if (kind == 1) {
-      q.ring = reinterpret_cast<uint32_t*>(h->base + L.vq_off) + static_cast<size_t>(c) * kVqSize;
-      q.ring_mask = kVqSize - 1u;
-      q.page_cap = kVqSize * kQcSpots;
+      q.ring = reinterpret_cast<uint32_t*>(h->base + L.vq_off) + static_cast<size_t>(c) * vq;
+      q.ring_mask = vq - 1u;
+      q.page_cap = vq * kQcSpots;
     } else {
       q.page_cap = 1u << 30;   // linked queues are unbounded; positions are 32-bit
       q.skip = reinterpret_cast<uint32_t*>(h->base + L.skip_off) + static_cast<size_t>(c) * kSkipSlots;
@@ -481,7 +514,8 @@ int ouro_state(ouro_heap* h, uint64_t* out) {
   }
   const int kind = h->variant / 2;
   const bool chunk_based = (h->variant % 2) == 1;
-  std::vector<uint32_t> vq(kVqSize);
+  const uint32_t vq_entries = static_cast<uint32_t>(h->L.vq_entries);
+  std::vector<uint32_t> vq(vq_entries);
   for (uint32_t c = 0; c < kNumClasses; ++c) {
     const ClassState& q = core.cls[c];
     uint64_t* o = out + 7 + 12 * c;
@@ -498,9 +532,9 @@ int ouro_state(ouro_heap* h, uint64_t* out) {
       o[9] = q.old_count;
     }
     if (kind == 1) {
-      if (cudaMemcpy(vq.data(), q.ring, kVqSize * 4u, cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
+      if (cudaMemcpy(vq.data(), q.ring, vq_entries * 4u, cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
       uint64_t d = 0;
-      for (uint32_t v = 0; v < kVqSize; ++v)
+      for (uint32_t v = 0; v < vq_entries; ++v)
         if (vq[v] != kEmpty) d += static_cast<uint64_t>(v + 1u) * (static_cast<uint64_t>(vq[v]) + 1u);
       o[10] = d;
     }

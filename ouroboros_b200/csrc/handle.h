@@ -14,6 +14,7 @@ struct ouro_heap {
   int device;
   unsigned long long heap_bytes;
   ouro::Layout L;
+  ouro_config cfg;
   void* raw;
   ouro::HeapCore* dev;
   char* base;

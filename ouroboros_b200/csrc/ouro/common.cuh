@@ -21,9 +21,10 @@ constexpr uint32_t kMetaBytes = 128u;
 constexpr uint32_t kRefStride = 8320u;      // reference chunk stride, capacity formula only
 constexpr uint32_t kNumClasses = 12u;       // 10 + 2
 constexpr uint32_t kQcSpots = 2048u;        // entries per queue chunk
+// Queue sizes: the reference's, the defaults of the run-time configuration
+// (each heap carries its own in ClassState::ring_mask / seg_mask).
 constexpr uint32_t kVqSize = 16384u;        // virtual-array index entries
 constexpr uint32_t kRingSize = 1u << 23;    // standard ring entries per class
-constexpr uint32_t kRingSegs = kRingSize / 2048u;   // standard chunk queues: removal counters per 2048 entries
 constexpr uint32_t kReuseSize = 65536u;     // chunk reuse ring
 constexpr uint32_t kOldHold = 10u;          // linked queue chunks held back before reuse
 constexpr int kLowerFillC = 838860;         // chunk flashing threshold of the standard chunk queue

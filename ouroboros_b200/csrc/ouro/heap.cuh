@@ -51,6 +51,7 @@ struct alignas(128) ClassState {
   int32_t holes;                  // semaphore: pages of failed chunk additions not yet handed back
   uint32_t* skip;                 // linked: index of recently linked queue chunks
   uint32_t* seg;                  // standard chunk queues: removed entries per 2048-entry ring segment
+  uint32_t seg_mask;              // standard chunk queues: ring segments - 1
 };
 
 struct alignas(128) ReuseQueue {
@@ -74,6 +75,7 @@ struct alignas(128) HeapCore {
   unsigned long long alloc_bytes;
   unsigned long long heap_bytes;
   unsigned long long budget_limit;     // virtualized: chunks the budget may commit (0: no budget)
+  uint32_t agg_width;                  // lanes per aggregation segment of a warp (1..32, a power of two)
   // hot / warm counters
   Line<unsigned long long> next_free_chunk;
   Line<uint32_t> status;
@@ -124,6 +126,8 @@ __device__ __forceinline__ void note_timeout(HeapCore* h, uint32_t site) {
 // own object and queue sizes, so that max_chunks (and with it every success /
 // failure count) is identical.  Physical placement is this build's own.
 struct Layout {
+  unsigned long long ring_entries;   // standard queues: ring entries per class
+  unsigned long long vq_entries;     // virtualized-array queues: index entries per class
   unsigned long long ref_queue_bytes;
   unsigned long long ref_total_required;
   unsigned long long max_chunks;
@@ -135,10 +139,14 @@ __host__ __device__ inline unsigned long long align_up(unsigned long long v, uns
   return (v + a - 1u) / a * a;
 }
 
-// kind: 0 standard, 1 virtualized array, 2 virtualized linked list
-__host__ inline bool compute_layout(int kind, unsigned long long heap_bytes, Layout* L) {
-  const unsigned long long per_queue = kind == 0 ? (unsigned long long)kRingSize * 4u
-                                     : kind == 1 ? (unsigned long long)kVqSize * 4u : 0u;
+// kind: 0 standard, 1 virtualized array, 2 virtualized linked list.  The queue
+// sizes default to the reference's (page_queue_size, virtual_queue_size).
+__host__ inline bool compute_layout(int kind, unsigned long long heap_bytes, Layout* L,
+                                    unsigned long long ring_entries = kRingSize,
+                                    unsigned long long vq_entries = kVqSize) {
+  L->ring_entries = ring_entries;
+  L->vq_entries = vq_entries;
+  const unsigned long long per_queue = kind == 0 ? ring_entries * 4u : kind == 1 ? vq_entries * 4u : 0u;
   const unsigned long long reuse = align_up((unsigned long long)kReuseSize * 4u, kChunkBytes);
   const unsigned long long pq = align_up(per_queue, kChunkBytes);
   L->ref_queue_bytes = reuse + pq * 10u + reuse + pq * 2u;
@@ -151,15 +159,15 @@ __host__ inline bool compute_layout(int kind, unsigned long long heap_bytes, Lay
   L->data_off = align_up(L->meta_off + L->max_chunks * kMetaBytes, kChunkBytes);
   unsigned long long off = L->data_off + L->max_chunks * kChunkBytes;
   L->ring_off = off;
-  if (kind == 0) off += (unsigned long long)kNumClasses * kRingSize * 4u;
+  if (kind == 0) off += (unsigned long long)kNumClasses * ring_entries * 4u;
   L->vq_off = off;
-  if (kind == 1) off += (unsigned long long)kNumClasses * kVqSize * 4u;
+  if (kind == 1) off += (unsigned long long)kNumClasses * vq_entries * 4u;
   L->skip_off = off;
   if (kind == 2) off += (unsigned long long)kNumClasses * kSkipSlots * 4u;
   L->reuse_off = off;
   off += 2ull * kReuseSize * 4u;
   L->seg_off = off;
-  if (kind == 0) off += (unsigned long long)kNumClasses * kRingSegs * 4u;
+  if (kind == 0) off += (unsigned long long)kNumClasses * (ring_entries / kQcSpots) * 4u;
   L->alloc_bytes = align_up(off, kChunkBytes) + kChunkBytes;   // + slack to 8 KiB-align the base
   return true;
 }

@@ -26,9 +26,17 @@ struct Ouroboros : HeapCore {
   static constexpr int kKind = V / 2;
   using Store = std::conditional_t<kKind == 0, FlatStore, std::conditional_t<kKind == 1, VaStore, VlStore>>;
 
+  // The lanes of this lane's aggregation segment (agg_width consecutive lanes;
+  // the whole warp by default): requests are aggregated within it only.
+  __device__ __forceinline__ uint32_t segment() const {
+    const uint32_t w = this->agg_width;
+    if (w - 1u >= 31u) return 0xFFFFFFFFu;   // 32 (or an unset 0): the whole warp
+    return ((1u << w) - 1u) << (lane_id() & ~(w - 1u));
+  }
+
   __device__ __forceinline__ void* malloc(size_t size) {
     const int cls = size_class(size);
-    const uint32_t active = __activemask();
+    const uint32_t active = __activemask() & segment();
     const Group g = group_by(active, static_cast<uint64_t>(cls + 1));
     if (cls < 0) {
       // Ouroboros<>::malloc: next power of two from the CUDA device heap
@@ -83,7 +91,7 @@ struct Ouroboros : HeapCore {
   }
 
   __device__ __forceinline__ void free(void* ptr) {
-    const uint32_t active = __activemask();
+    const uint32_t active = __activemask() & segment();
     char* p = static_cast<char*>(ptr);
     const bool in_heap = p >= this->data && p < this->data_end;
     const uint32_t heap_mask = __ballot_sync(active, in_heap);

@@ -194,14 +194,14 @@ __device__ __forceinline__ uint32_t rotr32(uint32_t m, uint32_t off) { return of
 __device__ __forceinline__ uint32_t rotl32(uint32_t m, uint32_t off) { return off ? __funnelshift_l(m, m, off) : m; }
 
 // Entries of the chunk queue: how many, against the queue capacity.
-__device__ __forceinline__ uint32_t chunk_queue_cap(int kind) {
-  return kind == 0 ? kRingSize : kind == 1 ? kVqSize * kQcSpots : 0xFFFFFFF0u;
+__device__ __forceinline__ uint32_t chunk_queue_cap(const ClassState* q, int kind) {
+  return kind == 2 ? 0xFFFFFFF0u : q->page_cap;
 }
 
 template <class Store>
 __device__ void chunk_enqueue(HeapCore* h, ClassState* q, uint32_t c) {
   int32_t fill = atomicAdd(&q->entries.v, 1);
-  if (static_cast<uint32_t>(fill) >= chunk_queue_cap(Store::kKind)) {
+  if (static_cast<uint32_t>(fill) >= chunk_queue_cap(q, Store::kKind)) {
     atomicSub(&q->entries.v, 1);
     st_relaxed(&h->meta[c].queue_pos, kEmpty);
     set_status(h, kErrQueueFull);
@@ -222,7 +222,7 @@ __device__ void chunk_enqueue_group(HeapCore* h, ClassState* q, const Group& g, 
   uint32_t b = 0, full = 0;
   if (g.is_leader()) {
     const int32_t fill = atomicAdd(&q->entries.v, static_cast<int32_t>(n));
-    if (static_cast<uint32_t>(fill) + n > chunk_queue_cap(Store::kKind)) {
+    if (static_cast<uint32_t>(fill) + n > chunk_queue_cap(q, Store::kKind)) {
       atomicSub(&q->entries.v, static_cast<int32_t>(n));
       set_status(h, kErrQueueFull);
       full = 1u;

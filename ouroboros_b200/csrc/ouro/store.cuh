@@ -134,7 +134,7 @@ struct FlatStore {
   // The removal is counted per 2048-entry segment of the ring after the
   // tombstone is written, so a count never runs ahead of the tombstones.
   __device__ static uint32_t* seg_count(ClassState* q, uint32_t pos) {
-    return q->seg + ((pos / 2048u) & (kRingSegs - 1u));
+    return q->seg + ((pos / 2048u) & q->seg_mask);
   }
   __device__ static bool remove(HeapCore* h, ClassState* q, uint32_t pos) {
     st_relaxed(slot(q, pos), kTomb);
@@ -223,11 +223,11 @@ struct FlatStore {
 struct VaStore {
   static constexpr int kKind = 1;
 
-  __device__ static uint32_t vid(uint32_t pos) { return (pos / kQcSpots) & (kVqSize - 1u); }
+  __device__ static uint32_t vid(const ClassState* q, uint32_t pos) { return (pos / kQcSpots) & q->ring_mask; }
 
   // The queue chunk holding pos (spins while its pre-allocation is in flight).
   __device__ static uint32_t qchunk(HeapCore* h, ClassState* q, uint32_t pos) {
-    uint32_t* e = q->ring + vid(pos);
+    uint32_t* e = q->ring + vid(q, pos);
     uint32_t c, it = 0;
     while ((c = ld_acquire(e)) == kEmpty || c == kInstalling) {
       if (it >= kSpinLimit) { note_timeout(h, kWaitIndexEntry); return kEmpty; }
@@ -245,12 +245,12 @@ struct VaStore {
   // The producer of a position at the start of a queue chunk allocates the
   // next queue chunk (PageQueueVA_impl.cuh:45-56, :202-212).
   __device__ static void preallocate(HeapCore* h, ClassState* q, uint32_t pos) {
-    offer_queue_chunk(h, q->ring + vid(pos + kQcSpots), new_queue_chunk(h, q->inst, pos + kQcSpots, queue_tag(q)));
+    offer_queue_chunk(h, q->ring + vid(q, pos + kQcSpots), new_queue_chunk(h, q->inst, pos + kQcSpots, queue_tag(q)));
   }
 
   // Drained queue chunk back to the chunk pool (PageQueueVA_impl.cuh:159-166).
   __device__ static void recycle(HeapCore* h, ClassState* q, uint32_t pos) {
-    uint32_t c = atomicExch(q->ring + vid(pos), kEmpty);
+    uint32_t c = atomicExch(q->ring + vid(q, pos), kEmpty);
     if (c < kInstalling) reuse_put(h, &h->reuse[0], c);
   }
 
@@ -356,13 +356,13 @@ struct VaStore {
   struct Cursor { uint32_t unused; };
   __device__ static Cursor cursor(ClassState*) { return Cursor{0}; }
   __device__ static uint32_t peek(HeapCore* h, ClassState* q, uint32_t pos, Cursor&) {
-    uint32_t qc = ld_acquire(q->ring + vid(pos));
+    uint32_t qc = ld_acquire(q->ring + vid(q, pos));
     if (qc >= kInstalling) return kEmpty;
     if (ld_relaxed(&h->meta[qc].vstart) / kQcSpots != pos / kQcSpots) return kTomb;
     return ld_acquire(queue_slots(h, qc) + (pos % kQcSpots));
   }
   __device__ static bool remove(HeapCore* h, ClassState* q, uint32_t pos) {
-    uint32_t qc = ld_acquire(q->ring + vid(pos));
+    uint32_t qc = ld_acquire(q->ring + vid(q, pos));
     if (qc >= kInstalling) return false;
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
     atomicSub(&h->meta[qc].qcount, 1u << 16);
@@ -396,7 +396,7 @@ struct VaStore {
         for (uint32_t k = 0; k < 64u; ++k) {
           const uint32_t rg = skip / kQcSpots, end = (rg + 1u) * kQcSpots;
           if (static_cast<int32_t>(end - back) > 0) break;
-          const uint32_t c = ld_acquire(q->ring + vid(skip));
+          const uint32_t c = ld_acquire(q->ring + vid(q, skip));
           if (c >= kInstalling || ld_relaxed(&h->meta[c].vstart) / kQcSpots != rg) break;
           if (ld_acquire(&h->meta[c].qcount) != kQcSpots) break;
           skip = end;
@@ -413,7 +413,7 @@ struct VaStore {
       if (static_cast<int32_t>(p - back) < 0) {
         if (p / kQcSpots != range) {
           range = p / kQcSpots;
-          qc = ld_acquire(q->ring + vid(p));
+          qc = ld_acquire(q->ring + vid(q, p));
           if (qc >= kInstalling || ld_relaxed(&h->meta[qc].vstart) / kQcSpots != range) qc = kEmpty;
         }
         if (qc != kEmpty) e = ld_relaxed_v4(queue_slots(h, qc) + (p % kQcSpots));
@@ -437,7 +437,7 @@ struct VaStore {
          end0 += n * kQcSpots) {
       const uint32_t end = end0 + static_cast<uint32_t>(g.rank) * kQcSpots;
       if (static_cast<int32_t>(stop - end) < 0) continue;
-      const uint32_t c = atomicExch(q->ring + vid(end - 1u), kEmpty);
+      const uint32_t c = atomicExch(q->ring + vid(q, end - 1u), kEmpty);
       if (c >= kInstalling) continue;
       uint32_t* slots = queue_slots(h, c);
       for (uint32_t i = 0; i < kQcSpots; i += 4u) st_v4(slots + i, empty);

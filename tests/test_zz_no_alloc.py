@@ -21,10 +21,12 @@ pytestmark = pytest.mark.gpu
 FIELDS = ("checked", "nulls", "out_of_heap", "misaligned", "overlaps")
 
 
-def _noalloc(heap, ptrs, n, sizes):
+def _noalloc(heap, ptrs, n, sizes, size=0, stream=None):
     rep = torch.full((5,), -1, dtype=torch.int64, device="cuda")   # garbage: the call must clear it
-    stream = torch.cuda.current_stream().cuda_stream
-    rc = ob.lib().ouro_check_allocations_noalloc(heap._handle(), ptrs.data_ptr(), n, 0, sizes.data_ptr(),
+    if stream is None:
+        stream = torch.cuda.current_stream().cuda_stream
+    rc = ob.lib().ouro_check_allocations_noalloc(heap._handle(), ptrs.data_ptr(), n, size,
+                                                 sizes.data_ptr() if sizes is not None else None,
                                                  rep.data_ptr(), stream)
     assert rc == 0, ob.lib().ouro_status_string(rc)
     torch.cuda.synchronize()
@@ -55,6 +57,46 @@ def test_noalloc_checker_matches_allocating_checker(v):
         assert _noalloc(heap, bad, n, sizes)["overlaps"] > 0
         heap.free(ptrs, n)
         torch.cuda.synchronize()
+
+
+# Heap sizes whose chunk data is exactly the scratch's limit of 131,072 chunks
+# (VAP layout), and one chunk more.
+AT_LIMIT_BYTES = 1091837824
+OVER_LIMIT_BYTES = AT_LIMIT_BYTES + 8320
+
+
+def test_noalloc_checker_uniform_size_at_the_limit():
+    """One size for every pointer (no size array), on a heap whose chunk data
+    is exactly the 8 MiB bitmap's reach.  A pointer to the heap's last chunk
+    puts bits into the bitmap's last words.  Two calls in a row on a side
+    stream, after one that left the array full of bits."""
+    with ob.Ouroboros("VAP", AT_LIMIT_BYTES) as heap:
+        assert heap.info()["max_chunks"] == 131072
+        n = 60000
+        ptrs = torch.zeros(n, dtype=torch.int64, device="cuda")
+        heap.alloc(ptrs, n, 8192)
+        torch.cuda.synchronize()
+        assert int((ptrs == 0).sum()) == 0
+        # the start of the heap's highest chunk: its 8 KiB are the bitmap's
+        # last 16 words
+        last = torch.tensor([heap.info()["data_end"] - 8192], dtype=torch.int64, device="cuda")
+        arr = torch.cat([ptrs, ptrs[:100], last])
+        side = torch.cuda.Stream()
+        for a in (arr, ptrs, ptrs):
+            want = heap.check_allocations(a, a.numel(), 8192)
+            with torch.cuda.stream(side):
+                got = _noalloc(heap, a, a.numel(), None, size=8192, stream=side.cuda_stream)
+            assert got == want
+        assert want == {"checked": n, "nulls": 0, "out_of_heap": 0, "misaligned": 0, "overlaps": 0}
+        heap.free(ptrs, n)
+        torch.cuda.synchronize()
+    with ob.Ouroboros("VAP", OVER_LIMIT_BYTES) as heap:
+        assert heap.info()["max_chunks"] == 131073
+        rep = torch.zeros(5, dtype=torch.int64, device="cuda")
+        ptrs = torch.zeros(4, dtype=torch.int64, device="cuda")
+        rc = ob.lib().ouro_check_allocations_noalloc(heap._handle(), ptrs.data_ptr(), 4, 16, None,
+                                                     rep.data_ptr(), None)
+        assert rc == 5
 
 
 def test_noalloc_checker_refuses_heaps_beyond_its_scratch():
