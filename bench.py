@@ -33,6 +33,10 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# Load every kernel's module when the context is created, not at its first
+# launch: otherwise the first (cold) repetition of each cell would include
+# loading the alloc/free kernels of its instantiation, in both arms.
+os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
 
 import numpy as np  # noqa: E402
 import torch  # noqa: E402

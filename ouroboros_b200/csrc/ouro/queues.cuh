@@ -254,7 +254,8 @@ __device__ void ensure_enqueued(HeapCore* h, ClassState* q, uint32_t c) {
 template <class Store>
 __device__ void help_front(HeapCore* h, ClassState* q, const Group& g) {
   uint32_t mine = 0;
-  if (g.is_leader()) mine = atomicCAS(&q->advancing.v, 0u, 1u) == 0u ? 1u : 0u;
+  // test before the CAS: while one group moves the front, the others only read the line
+  if (g.is_leader() && ld_relaxed(&q->advancing.v) == 0u) mine = atomicCAS(&q->advancing.v, 0u, 1u) == 0u ? 1u : 0u;
   if (!bcast(g, mine)) return;
   Store::advance_front(h, q, g);
   __syncwarp(g.mask);
@@ -268,10 +269,12 @@ __device__ void help_front(HeapCore* h, ClassState* q, const Group& g) {
 // ChunkQueue_impl.cuh:128-137).  Called by one lane; returns kRemoved when it
 // removed the entry, after which its group should help the front, plus
 // kDrainedQc when the removal drained a queue chunk, after which its group
-// runs Store::after_drain.
+// runs Store::after_drain.  count = false leaves the class's entry count to
+// the caller, which lowers it once for all removals of its group (the count
+// line is shared by every group of the class).
 constexpr uint32_t kRemoved = 1u, kDrainedQc = 2u;
 template <class Store>
-__device__ uint32_t chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos) {
+__device__ uint32_t chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos, bool count = true) {
   uint32_t* qp = &h->meta[c].queue_pos;
   uint32_t it = 0;
   while (ld_relaxed(qp) == kPending) {
@@ -280,7 +283,7 @@ __device__ uint32_t chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32
   }
   if (atomicCAS(qp, pos, kEmpty) != pos) return 0u;   // someone else removed or moved it
   const bool drained = Store::remove(h, q, pos);
-  atomicSub(&q->entries.v, 1);
+  if (count) atomicSub(&q->entries.v, 1);
   __threadfence();
   if (ld_relaxed(&h->meta[c].count) > 0) ensure_enqueued<Store>(h, q, c);
   return kRemoved | (drained ? kDrainedQc : 0u);
@@ -486,9 +489,11 @@ __device__ void chunk_alloc_run(HeapCore* h, ClassState* q, const Group& s, type
       if (served && !was) chunk = c;
     }
   }
-  const uint32_t rf = last ? chunk_dequeue<Store>(h, q, v, pos) : 0u;
+  const uint32_t rf = last ? chunk_dequeue<Store>(h, q, v, pos, false) : 0u;
+  const uint32_t removed = __ballot_sync(s.mask, rf != 0u);
+  if (removed && s.is_leader()) atomicSub(&q->entries.v, __popc(removed));
   if (__ballot_sync(s.mask, (rf & kDrainedQc) != 0u)) Store::after_drain(h, q, s);
-  if (__ballot_sync(s.mask, rf != 0u)) help_front<Store>(h, q, s);
+  if (removed) help_front<Store>(h, q, s);
 }
 
 // ChunkQueue_impl.cuh:82-148 allocPage, for a group.  The first probe is the
