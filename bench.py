@@ -735,6 +735,19 @@ def batched_bench(n: int, cycles: int, stream) -> dict:
     flush = torch.zeros(64 << 20, dtype=torch.int32, device="cuda")
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     out = {"workload": "VAC, 8 GiB heap, %d requests log-uniform 16..8192 B (rounded up to 16 B)" % n}
+    # the run-time configuration: queue capacity x aggregation width x block
+    # size, each candidate on a fresh heap (ouro_autotune_config)
+    try:
+        tc = ob.autotune_config("VAC", 8 * GiB, min(n, 1 << 20), 16, 8192, reps=2)
+        pts = tc["points"]
+        dflt = [p for p in pts if p["virtual_queue_entries"] == 512 and p["agg_width"] == 32]
+        out["autotune_config"] = {
+            "best": tc["best"], "candidates": len(pts), "accepted": sum(p["ok"] for p in pts),
+            "swept": {"queue_entries_per_class": [1 << 16, 1 << 17, 1 << 18, 1 << 19, 1 << 20],
+                      "agg_width": [8, 16, 32], "block": [128, 256, 512, 1024]},
+            "best_at_2e20_entries_agg32": max((p["mops"] for p in dflt if p["ok"]), default=None)}
+    except Exception as exc:   # reported, the rest stands
+        out["autotune_config"] = {"error": str(exc)[:300]}
     with ob.Ouroboros("VAC", 8 * GiB) as heap:
         out["autotune"] = heap.autotune_batch(n=min(n, 1 << 20), lo=16, hi=8192)
         res = {}

@@ -228,8 +228,8 @@ __global__ void k_check_heap(const HeapCore* h, uint64_t nchunks, bool chunk_bas
     for (uint32_t w = 0; w < words; ++w) {
       const uint32_t lo = w * 32u;
       const uint32_t valid = m->size >= lo + 32u ? 0xFFFFFFFFu : (m->size > lo ? ((1u << (m->size - lo)) - 1u) : 0u);
-      ones += __popc(m->mask[w] & valid);
-      stray += __popc(m->mask[w] & ~valid);
+      ones += __popc(*m->mask(w) & valid);
+      stray += __popc(*m->mask(w) & ~valid);
     }
     if (m->count >= 0) atomicAdd(&r[12 + cls], static_cast<unsigned long long>(m->count));
     if (stray || static_cast<int32_t>(ones) != m->count) atomicAdd(&r[25], 1ull);

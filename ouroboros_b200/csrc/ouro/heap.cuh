@@ -10,17 +10,26 @@ namespace ouro {
 // role at a time: page chunk (page-based variants), chunk-index chunk
 // (chunk-based variants: free-page count + occupancy bitmask) or queue chunk
 // (2048 queue entries of the virtualized variants, stored in its data).
+// The first 32 B sector holds what an allocation of a chunk-based class with
+// at most 128 pages per chunk touches: the header, the free count and the
+// first four mask words; the queue fields follow in the same 64 B half, so a
+// request of 64 B or more reads the record from DRAM once, in one piece.
 struct alignas(128) ChunkMeta {
   uint32_t page_size;   // data chunks: page size of their class; 0 otherwise
   uint32_t head;        // >0: continuation of a 4-chunk chunk starting `head` chunks lower
   uint32_t size;        // pages in the chunk
   int32_t count;        // chunk-based: free pages (may dip below 0 transiently)
+  uint32_t mask_lo[4];  // chunk-based: mask words 0..3 (one bit per page, 1 = free)
   uint32_t queue_pos;   // chunk-based: virtual position of its queue entry, kEmpty or kPending
   uint32_t qcount;      // queue chunk: present << 16 | enqueued
   uint32_t vstart;      // queue chunk: first virtual position stored here
   uint32_t next;        // linked queue chunk: next queue chunk, kEmpty if none yet
-  uint32_t reserved_[8];
-  uint32_t mask[16];    // chunk-based: one bit per page, 1 = free
+  uint32_t reserved_[4];
+  uint32_t mask_hi[12]; // chunk-based: mask words 4..15 (pages 128..511 of the 16 B class)
+  uint32_t reserved2_[4];
+  // mask word w (0..15)
+  __host__ __device__ uint32_t* mask(uint32_t w) { return w < 4u ? mask_lo + w : mask_hi + (w - 4u); }
+  __host__ __device__ const uint32_t* mask(uint32_t w) const { return w < 4u ? mask_lo + w : mask_hi + (w - 4u); }
 };
 static_assert(sizeof(ChunkMeta) == 128, "metadata record must be one 128 B line");
 

@@ -29,7 +29,7 @@ __device__ __forceinline__ void init_data_chunk(HeapCore* h, ClassState* q, uint
     uint32_t n = q->ppc;
 #pragma unroll
     for (uint32_t w = 0; w < 16u; ++w) {
-      st_relaxed(&m->mask[w], n >= 32u ? 0xFFFFFFFFu : ((1u << n) - 1u));
+      st_relaxed(m->mask(w), n >= 32u ? 0xFFFFFFFFu : ((1u << n) - 1u));
       n = n > 32u ? n - 32u : 0u;
     }
     __threadfence();
@@ -272,17 +272,23 @@ __device__ void help_front(HeapCore* h, ClassState* q, const Group& g) {
 // runs Store::after_drain.  count = false leaves the class's entry count to
 // the caller, which lowers it once for all removals of its group (the count
 // line is shared by every group of the class).
+// `at` is the cursor of the peek that found the entry: the queue chunk holding
+// pos, which cannot drain before this removal, so the store need not find it
+// again.
 constexpr uint32_t kRemoved = 1u, kDrainedQc = 2u;
 template <class Store>
-__device__ uint32_t chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos, bool count = true) {
+__device__ uint32_t chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos, bool count = true,
+                                  const typename Store::Cursor* at = nullptr) {
   uint32_t* qp = &h->meta[c].queue_pos;
-  uint32_t it = 0;
-  while (ld_relaxed(qp) == kPending) {
+  // the CAS first: only an enqueue in flight (kPending) is waited for
+  uint32_t seen = atomicCAS(qp, pos, kEmpty);
+  for (uint32_t it = 0; seen == kPending;) {
     if (it >= 4096u) return 0u;
     backoff(it);
+    seen = atomicCAS(qp, pos, kEmpty);
   }
-  if (atomicCAS(qp, pos, kEmpty) != pos) return 0u;   // someone else removed or moved it
-  const bool drained = Store::remove(h, q, pos);
+  if (seen != pos) return 0u;   // someone else removed or moved it
+  const bool drained = Store::remove(h, q, pos, at);
   if (count) atomicSub(&q->entries.v, 1);
   __threadfence();
   if (ld_relaxed(&h->meta[c].count) > 0) ensure_enqueued<Store>(h, q, c);
@@ -307,13 +313,13 @@ __device__ void claim_pages(HeapCore* h, const Group& s, uint32_t c, uint32_t go
       const uint32_t w = (start + j) % W;
       uint32_t won = 0;
       if (s.is_leader()) {
-        const uint32_t rot = rotr32(ld_relaxed(&m->mask[w]), offset);
+        const uint32_t rot = rotr32(ld_relaxed(m->mask(w)), offset);
         const uint32_t avail = static_cast<uint32_t>(__popc(rot));
         const uint32_t take = avail < remaining ? avail : remaining;
         if (take) {
           const uint32_t p = __fns(rot, 0u, static_cast<int>(take));
           const uint32_t picked = rotl32(rot & ((2u << p) - 1u), offset);
-          won = picked & atomicAnd(&m->mask[w], ~picked);
+          won = picked & atomicAnd(m->mask(w), ~picked);
         }
       }
       won = bcast(s, won);
@@ -450,7 +456,7 @@ __device__ void chunk_alloc_run(HeapCore* h, ClassState* q, const Group& s, type
     // rank order by a prefix sum over them.
     uint32_t won = 0;
     if (got) {
-      uint32_t* mw = &h->meta[v].mask[0];
+      uint32_t* mw = h->meta[v].mask(0);
       uint32_t remaining = got;
       for (uint32_t attempt = 0; attempt < 64u && remaining; ++attempt) {
         const uint32_t w = ld_relaxed(mw);
@@ -489,7 +495,7 @@ __device__ void chunk_alloc_run(HeapCore* h, ClassState* q, const Group& s, type
       if (served && !was) chunk = c;
     }
   }
-  const uint32_t rf = last ? chunk_dequeue<Store>(h, q, v, pos, false) : 0u;
+  const uint32_t rf = last ? chunk_dequeue<Store>(h, q, v, pos, false, &cur) : 0u;
   const uint32_t removed = __ballot_sync(s.mask, rf != 0u);
   if (removed && s.is_leader()) atomicSub(&q->entries.v, __popc(removed));
   if (__ballot_sync(s.mask, (rf & kDrainedQc) != 0u)) Store::after_drain(h, q, s);
@@ -618,7 +624,7 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
       if (served && !before) chunk = c;
       uint32_t removed = 0;
       if (s.is_leader()) {
-        if (last) removed = chunk_dequeue<Store>(h, q, c, pos);
+        if (last) removed = chunk_dequeue<Store>(h, q, c, pos, true, &cur);
         ++pos;
       }
       removed = bcast(s, removed);
@@ -715,7 +721,7 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
   Group wg = group_by(cg.mask, page >> 5);
   uint32_t bits = __reduce_or_sync(wg.mask, 1u << (page & 31u));
   ChunkMeta* m = h->meta + c;
-  if (wg.is_leader()) atomicOr(&m->mask[page >> 5], bits);
+  if (wg.is_leader()) atomicOr(m->mask(page >> 5), bits);
   __syncwarp(cg.mask);
   __threadfence();
   uint32_t flashed = 0, help = 0, enq = 0, drained = 0;
@@ -814,7 +820,7 @@ __device__ bool enqueue_initial(HeapCore* h, ClassState* q, uint32_t c, uint32_t
     for (uint32_t w = 0; w < 16u; ++w) {
       const uint32_t full = n >= 32u ? 0xFFFFFFFFu : ((1u << n) - 1u);
       const uint32_t used = taken >= 32u ? 0xFFFFFFFFu : ((1u << taken) - 1u);
-      st_relaxed(&m->mask[w], full & ~used);
+      st_relaxed(m->mask(w), full & ~used);
       n = n > 32u ? n - 32u : 0u;
       taken = taken > 32u ? taken - 32u : 0u;
     }

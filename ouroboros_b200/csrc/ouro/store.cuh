@@ -136,7 +136,7 @@ struct FlatStore {
   __device__ static uint32_t* seg_count(ClassState* q, uint32_t pos) {
     return q->seg + ((pos / 2048u) & q->seg_mask);
   }
-  __device__ static bool remove(HeapCore* h, ClassState* q, uint32_t pos) {
+  __device__ static bool remove(HeapCore* h, ClassState* q, uint32_t pos, const Cursor* = nullptr) {
     st_relaxed(slot(q, pos), kTomb);
     __threadfence();
     atomicAdd(seg_count(q, pos), 1u);
@@ -353,16 +353,22 @@ struct VaStore {
     atomicAdd(&h->meta[qc].qcount, (1u << 16) + 1u);
     return true;
   }
-  struct Cursor { uint32_t unused; };
-  __device__ static Cursor cursor(ClassState*) { return Cursor{0}; }
-  __device__ static uint32_t peek(HeapCore* h, ClassState* q, uint32_t pos, Cursor&) {
+  // the queue chunk of the last position peeked at
+  struct Cursor { uint32_t chunk; };
+  __device__ static Cursor cursor(ClassState*) { return Cursor{kEmpty}; }
+  __device__ static uint32_t peek(HeapCore* h, ClassState* q, uint32_t pos, Cursor& cur) {
     uint32_t qc = ld_acquire(q->ring + vid(q, pos));
+    cur.chunk = kEmpty;
     if (qc >= kInstalling) return kEmpty;
     if (ld_relaxed(&h->meta[qc].vstart) / kQcSpots != pos / kQcSpots) return kTomb;
+    cur.chunk = qc;
     return ld_acquire(queue_slots(h, qc) + (pos % kQcSpots));
   }
-  __device__ static bool remove(HeapCore* h, ClassState* q, uint32_t pos) {
-    uint32_t qc = ld_acquire(q->ring + vid(q, pos));
+  // at: the cursor of the peek that found pos's entry, which the caller is
+  // removing; its queue chunk cannot drain or be reused before this removal.
+  __device__ static bool remove(HeapCore* h, ClassState* q, uint32_t pos, const Cursor* at = nullptr) {
+    uint32_t qc = at ? at->chunk : kEmpty;
+    if (qc == kEmpty) qc = ld_acquire(q->ring + vid(q, pos));
     if (qc >= kInstalling) return false;
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
     atomicSub(&h->meta[qc].qcount, 1u << 16);
@@ -1008,8 +1014,11 @@ struct VlStore {
   // Returns true when this removal drained the queue chunk: the caller's
   // group then runs after_drain (on_empty), so that front_ptr moves with a
   // whole group's walk rather than one lane's.
-  __device__ static bool remove(HeapCore* h, ClassState* q, uint32_t pos) {
-    uint32_t qc = locate_live(h, q, &q->front_ptr, pos);
+  // at: the cursor of the peek that found pos's entry (see VaStore::remove).
+  __device__ static bool remove(HeapCore* h, ClassState* q, uint32_t pos, const Cursor* at = nullptr) {
+    uint32_t qc = at ? at->chunk : kEmpty;
+    if (qc == kEmpty || ld_relaxed(&h->meta[qc].vstart) / kQcSpots != pos / kQcSpots)
+      qc = locate_live(h, q, &q->front_ptr, pos);
     if (qc == kEmpty || qc == kBehind) return false;
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
     __threadfence();
