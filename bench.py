@@ -680,6 +680,7 @@ def roofline(res, n, steps) -> dict:
     groups = n / 32.0
     hot_achieved = hot_lines * groups / (avg_ms * 1e-3) / 1e9
     hot = ob.measure_atomics(1)
+    two_lines = {"one_256B_block": ob.measure_atomics(3), "separate_256B_blocks": ob.measure_atomics(4)}
     distinct = ob.measure_atomics(0)
     vidx = VARIANTS.index(v)
     traffic, traffic_cell = None, None
@@ -711,7 +712,10 @@ def roofline(res, n, steps) -> dict:
             "rmw_per_launch": hot_lines * groups, "achieved_gops": round(hot_achieved, 4),
             "peak_gops": round(hot_lines * hot, 4),
             "peak_source": f"measured live: one hot 32-bit address, one RMW per warp, x{hot_lines} independent lines",
-            "frac": round(hot_achieved / (hot_lines * hot), 4)},
+            "frac": round(hot_achieved / (hot_lines * hot), 4),
+            "two_hot_lines_gops": {k: round(x, 4) for k, x in two_lines.items()},
+            "note": "two hot lines in one 256 B block share an L2 slice; the allocator's hot counters each "
+                    "have a 256 B block of their own"},
         "hbm": {"bytes_per_launch": 16.0 * n, "achieved_gbs": round(16.0 * n / (avg_ms * 1e-3) / 1e9, 2),
                 "peak_gbs": hbm_peak, "peak_source": hbm_source,
                 "frac": round(16.0 * n / (avg_ms * 1e-3) / 1e9 / hbm_peak, 5),

@@ -425,8 +425,10 @@ int ouro_free_resources(ouro_heap* h, ouro_free_report* out);
 /* Measured L2 atomic throughput of the current device, the roofline
  * reference of the allocator kernels (no counterpart in the reference):
  * mode 0 distinct addresses (atomics/s over all lanes), mode 1 one hot 32-bit
- * address, mode 2 one hot 64-bit address (requests/s, one per warp).  Result
- * in G operations per second. */
+ * address, mode 2 one hot 64-bit address (requests/s, one per warp), modes 3
+ * and 4 two hot 32-bit addresses 128 B apart (one 256 B block) and 256 B apart,
+ * alternate warps on each (requests/s in total).  Result in G operations per
+ * second. */
 int ouro_measure_atomics(int mode, double* gops);
 
 /* Diagnostic counters, 12 words.  Chunk-based heaps: groups, probes, misses,

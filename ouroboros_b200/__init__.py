@@ -410,7 +410,8 @@ def verify_pattern(ptrs, n: int, counters, size: int = 0, seed: int = 0x9E3779B9
 
 
 def measure_atomics(mode: int) -> float:
-    """G L2 atomic operations per second: 0 distinct addresses, 1 / 2 one hot 32 / 64-bit address."""
+    """G L2 atomic operations per second: 0 distinct addresses, 1 / 2 one hot 32 / 64-bit address,
+    3 / 4 two hot 32-bit addresses 128 B / 256 B apart."""
     out = ctypes.c_double()
     _check(lib().ouro_measure_atomics(mode, ctypes.byref(out)), "ouro_measure_atomics")
     return float(out.value)

@@ -6,6 +6,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -248,12 +249,15 @@ __global__ void k_peak_distinct(uint32_t* a, uint32_t mask, int iters, uint32_t*
   for (int i = 0; i < iters; ++i) acc += atomicAdd(&a[(t + static_cast<uint32_t>(i) * stride) & mask], 1u);
   if (acc == 0x9E3779B9u) *sink = acc;
 }
-__global__ void k_peak_hot(uint32_t* a, unsigned long long* a64, int iters, int wide, uint32_t* sink) {
+// stride > 0: two hot addresses `stride` words apart, alternate warps on each
+// (mode 3: 128 B apart, one 256 B block; mode 4: 256 B apart).
+__global__ void k_peak_hot(uint32_t* a, unsigned long long* a64, int iters, int wide, uint32_t stride, uint32_t* sink) {
   if ((threadIdx.x & 31u) != 0u) return;
+  uint32_t* p = a + (((blockIdx.x * blockDim.x + threadIdx.x) >> 5) & 1u) * stride;
   uint32_t acc = 0;
   for (int i = 0; i < iters; ++i) {
     if (wide) acc += static_cast<uint32_t>(atomicAdd(a64, 32ull));
-    else acc += atomicAdd(a, 32u);
+    else acc += atomicAdd(p, 32u);
   }
   if (acc == 0x9E3779B9u) *sink = acc;
 }
@@ -353,7 +357,8 @@ int ouro_create_config(int variant, uint64_t heap_bytes, const ouro_config* cfg_
   const uint32_t ring = static_cast<uint32_t>(L.ring_entries), vq = static_cast<uint32_t>(L.vq_entries);
   const uint32_t segs = ring / kQcSpots;
   if (e == cudaSuccess && variant / 2 == 0) e = cudaMemset(h->base + L.seg_off, 0, kNumClasses * segs * 4ull);
-  HeapCore core;
+  std::unique_ptr<HeapCore> core_buf(new HeapCore());   // ~0.5 MiB: not on the stack
+  HeapCore& core = *core_buf;
   std::memset(&core, 0, sizeof(core));
   core.variant = variant;
   core.max_chunks = static_cast<uint32_t>(L.max_chunks);
@@ -503,7 +508,8 @@ int ouro_trace(ouro_heap* h, const uint32_t* ops, uint64_t n_ops, uint64_t* resu
 int ouro_state(ouro_heap* h, uint64_t* out) {
   if (!h || !out) return OURO_ERR_ARG;
   if (cudaDeviceSynchronize() != cudaSuccess) return OURO_ERR_CUDA;
-  HeapCore core;
+  std::unique_ptr<HeapCore> core_buf(new HeapCore());   // ~0.5 MiB: not on the stack
+  HeapCore& core = *core_buf;
   if (cudaMemcpy(&core, h->dev, sizeof(core), cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
   std::memset(out, 0, 151 * sizeof(uint64_t));
   out[0] = core.next_free_chunk.v;
@@ -546,7 +552,8 @@ int ouro_state(ouro_heap* h, uint64_t* out) {
 int ouro_get_status(ouro_heap* h, ouro_heap_status* out, int clear) {
   if (!h || !out) return OURO_ERR_ARG;
   if (cudaDeviceSynchronize() != cudaSuccess) return OURO_ERR_CUDA;
-  HeapCore core;
+  std::unique_ptr<HeapCore> core_buf(new HeapCore());   // ~0.5 MiB: not on the stack
+  HeapCore& core = *core_buf;
   if (cudaMemcpy(&core, h->dev, sizeof(core), cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
   out->flags = core.status.v;
   out->null_results = core.oom.v;
@@ -612,7 +619,8 @@ int ouro_check_allocations(ouro_heap* h, void* const* d_ptrs, uint32_t n, uint32
 int ouro_check_heap(ouro_heap* h, ouro_heap_report* out) {
   if (!h || !out) return OURO_ERR_ARG;
   if (cudaDeviceSynchronize() != cudaSuccess) return OURO_ERR_CUDA;
-  HeapCore core;
+  std::unique_ptr<HeapCore> core_buf(new HeapCore());   // ~0.5 MiB: not on the stack
+  HeapCore& core = *core_buf;
   if (cudaMemcpy(&core, h->dev, sizeof(core), cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
   uint64_t nchunks = core.next_free_chunk.v < h->L.max_chunks ? core.next_free_chunk.v : h->L.max_chunks;
   unsigned long long* r = nullptr;
@@ -711,7 +719,8 @@ int ouro_enqueue_initial_chunk(ouro_heap* h, uint32_t queue_index, uint32_t chun
 int ouro_free_resources(ouro_heap* h, ouro_free_report* out) {
   if (!h || !out) return OURO_ERR_ARG;
   if (cudaDeviceSynchronize() != cudaSuccess) return OURO_ERR_CUDA;
-  HeapCore core;
+  std::unique_ptr<HeapCore> core_buf(new HeapCore());   // ~0.5 MiB: not on the stack
+  HeapCore& core = *core_buf;
   if (cudaMemcpy(&core, h->dev, sizeof(core), cudaMemcpyDeviceToHost) != cudaSuccess) return OURO_ERR_CUDA;
   std::memset(out, 0, sizeof(*out));
   unsigned long long free_bytes = 0;
@@ -748,7 +757,7 @@ int ouro_scan_stats(ouro_heap* h, uint64_t* out, int clear) {
 }
 
 int ouro_measure_atomics(int mode, double* gops) {
-  if (!gops || mode < 0 || mode > 2) return OURO_ERR_ARG;
+  if (!gops || mode < 0 || mode > 4) return OURO_ERR_ARG;
   int sms = 0, dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return OURO_ERR_CUDA;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -765,7 +774,7 @@ int ouro_measure_atomics(int mode, double* gops) {
   const int iters = mode == 0 ? 64 : 16;
   auto launch = [&]() {
     if (mode == 0) k_peak_distinct<<<grid, block>>>(a, N - 1u, iters, sink);
-    else k_peak_hot<<<grid, block>>>(a, a64, iters, mode == 2, sink);
+    else k_peak_hot<<<grid, block>>>(a, a64, iters, mode == 2, mode == 3 ? 32u : mode == 4 ? 64u : 0u, sink);
   };
   launch();
   cudaEventRecord(e0);

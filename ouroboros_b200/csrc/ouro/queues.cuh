@@ -64,17 +64,24 @@ __device__ __forceinline__ uint32_t reserve_class_pages(HeapCore* h, ClassState*
 // it the last data chunks would leave no queue chunk for the entries they
 // bring, and producers would wait for a link that cannot come.  The queue of
 // the class grows from e0 entries by `per` entries per chunk; returns how
-// many of the k chunks (factor base chunks each) the class may add.
+// many of the k chunks (factor base chunks each) the class may add.  A claim
+// that overshoots the limit is undone at once, so near the limit another
+// group can see the budget spent while that claim is only passing through:
+// a group that meets it spent looks again a few times (about 3 us in all)
+// before it gives up.
 __device__ __forceinline__ uint32_t queue_chunks_for(uint32_t entries) { return (entries + kQcSpots - 1u) / kQcSpots; }
 
 __device__ inline uint32_t commit_budget(HeapCore* h, uint32_t k, uint32_t factor, uint32_t e0, uint32_t per) {
-  if (ld_relaxed(&h->budget.v) + factor > h->budget_limit) return 0u;   // spent: no atomics
-  for (uint32_t kk = k; kk; kk >>= 1) {
-    const unsigned long long d = static_cast<unsigned long long>(kk) * factor + queue_chunks_for(e0 + kk * per) -
-                                 queue_chunks_for(e0);
-    const unsigned long long old = atomicAdd(&h->budget.v, d);
-    if (old + d <= h->budget_limit) return kk;
-    atomicAdd(&h->budget.v, 0ull - d);
+  for (uint32_t look = 0, it = 0; look < 8u; ++look) {
+    if (look) backoff(it);
+    if (ld_relaxed(&h->budget.v) + factor > h->budget_limit) continue;   // spent for now: no atomics
+    for (uint32_t kk = k; kk; kk >>= 1) {
+      const unsigned long long d = static_cast<unsigned long long>(kk) * factor + queue_chunks_for(e0 + kk * per) -
+                                   queue_chunks_for(e0);
+      const unsigned long long old = atomicAdd(&h->budget.v, d);
+      if (old + d <= h->budget_limit) return kk;
+      atomicAdd(&h->budget.v, 0ull - d);
+    }
   }
   return 0u;
 }
