@@ -808,43 +808,73 @@ struct VlStore {
   // A producer at the start of a queue chunk links the next one
   // (QueueChunk_impl.cuh:144-158).  A link needs its predecessor, so linking
   // is a chain.  When producers already hold positions several queue chunks
-  // ahead (a burst), the group links a piece of up to kPieceRounds chunks per
-  // lane at once: one reservation of chunks, headers and links written in
-  // parallel, one CAS to attach the piece, and index entries written right
-  // after, so that waiting producers find their chunk in the index instead of
-  // walking.  The producer at the start of the piece's last range continues
-  // the chain, so a burst of B queue chunks waits for B / (kPieceRounds x 32)
-  // links in a row.  The piece is only ever attached to c, whose range the
-  // caller holds a position of: c cannot drain meanwhile.  (A chunk the
-  // caller does not hold may be drained, recycled and reused with an empty
-  // link, and a piece attached there would duplicate ranges of the live
-  // chain.)  A lone producer is never more than one chunk ahead, so it links
+  // ahead (a burst), the group links pieces of up to kPieceRounds chunks per
+  // lane: one reservation of chunks, headers and links written in parallel,
+  // one CAS to attach the piece, and index entries written right after, so
+  // that waiting producers find their chunk in the index instead of walking.
+  // Up to kPieceSegments pieces follow one another in one call, each attached
+  // to the last chunk of the one before, so a burst of up to
+  // kPieceSegments x kPieceRounds x 32 queue chunks (2^20 entries) is linked by
+  // one group without waiting for the producers further on.  The first piece
+  // is only ever attached to c, whose range the caller holds a position of: c
+  // cannot drain meanwhile.  (A chunk the caller does not hold may be
+  // drained, recycled and reused with an empty link, and a piece attached
+  // there would duplicate ranges of the live chain.)  Each further piece goes
+  // after the group's own newest chunk, whose link is still empty: front_ptr
+  // cannot pass a chunk without a successor, so that chunk is not recycled
+  // either.  A lone producer is never more than one chunk ahead, so it links
   // exactly one chunk, as the reference does.  c holds the range starting at
   // pos.  Collective over g.
+  // Segments: pieces one call may link (the page queues' producers use
+  // kPieceSegments; the chunk queues, whose bursts bring at most one entry per
+  // chunk, one: it keeps the allocation kernels' code small).
   static constexpr int kPieceRounds = 4;
+  static constexpr uint32_t kPieceSegments = 4u;
+  template <uint32_t Segments = 1u>
   __device__ static void preallocate(HeapCore* h, ClassState* q, const Group& g, uint32_t c, uint32_t pos) {
-    uint32_t* link = &h->meta[c].next;
     const uint32_t n = static_cast<uint32_t>(g.size), r = static_cast<uint32_t>(g.rank);
     uint32_t ahead = 0;
-    if (g.is_leader() && ld_relaxed(link) == kEmpty) {
+    if (g.is_leader() && ld_relaxed(&h->meta[c].next) == kEmpty) {
       const uint32_t back = ld_relaxed(&q->back.v);
       ahead = static_cast<int32_t>(back - pos) > static_cast<int32_t>(2u * kQcSpots)
                   ? (back - pos) / kQcSpots - 1u : 1u;
-      if (ahead > kPieceRounds * n) ahead = kPieceRounds * n;
+      if (ahead > Segments * kPieceRounds * n) ahead = Segments * kPieceRounds * n;
     }
     ahead = bcast(g, ahead);
-    if (!ahead) return;
+    if constexpr (Segments == 1u) {
+      if (ahead) link_piece<false>(h, q, g, c, pos, ahead);
+      return;
+    }
+    while (ahead) {
+      const uint32_t part = ahead < kPieceRounds * n ? ahead : kPieceRounds * n;
+      const uint32_t last = link_piece<true>(h, q, g, c, pos, part);
+      if (last == kEmpty) return;   // a shorter piece, none, or someone else linked c
+      ahead -= part;
+      c = last;
+      pos += part * kQcSpots;
+    }
+  }
+
+  // One piece of `part` queue chunks after c (range starting at pos).  Tail:
+  // return the piece's last chunk when the whole piece was attached (kEmpty
+  // otherwise); without Tail, kEmpty.
+  template <bool Tail>
+  __device__ static uint32_t link_piece(HeapCore* h, ClassState* q, const Group& g, uint32_t c, uint32_t pos,
+                                        uint32_t part) {
+    uint32_t* link = &h->meta[c].next;
+    const uint32_t n = static_cast<uint32_t>(g.size), r = static_cast<uint32_t>(g.rank);
     uint32_t mine[kPieceRounds];
-    const uint32_t got = alloc_chunk_rounds<kPieceRounds>(h, g, ahead, q->inst, true, mine);
+    const uint32_t got = alloc_chunk_rounds<kPieceRounds>(h, g, part, q->inst, true, mine);
     // the piece is the prefix of chunks up to the first one missing
-    uint32_t hole = ahead;
+    uint32_t hole = part;
 #pragma unroll
     for (int j = 0; j < kPieceRounds; ++j) {
       const uint32_t i = static_cast<uint32_t>(j) * n + r;
-      if (i < ahead && (i >= got || mine[j] == kEmpty) && i < hole) hole = i;
+      if (i < part && (i >= got || mine[j] == kEmpty) && i < hole) hole = i;
     }
     const uint32_t L = __reduce_min_sync(g.mask, hole);
     const int next_lane = lane_of_rank(g.mask, r + 1u < n ? static_cast<int>(r) + 1 : static_cast<int>(r));
+    uint32_t tail = kEmpty;   // the piece's last chunk, on the lane that holds it
 #pragma unroll
     for (int j = 0; j < kPieceRounds; ++j) {
       const uint32_t i = static_cast<uint32_t>(j) * n + r;
@@ -853,13 +883,14 @@ struct VlStore {
       if (i < L) {
         init_queue_chunk(h, mine[j], pos + (i + 1u) * kQcSpots, queue_tag(q));
         if (i + 1u < L) st_relaxed(&h->meta[mine[j]].next, r + 1u < n ? succ_same : succ_next);
+        else if constexpr (Tail) tail = mine[j];
       } else if (i < got && mine[j] != kEmpty) {
         reuse_put(h, &h->reuse[0], mine[j]);   // behind a hole: not part of the piece
       }
     }
     __threadfence();
     __syncwarp(g.mask);
-    if (L == 0u) return;
+    if (L == 0u) return kEmpty;
     const uint32_t piece = __shfl_sync(g.mask, mine[0], g.leader);
     uint32_t ok = 0;
     if (g.is_leader()) ok = atomicCAS(link, kEmpty, piece) == kEmpty ? 1u : 0u;
@@ -876,6 +907,8 @@ struct VlStore {
         reuse_put(h, &h->reuse[0], mine[j]);
       }
     }
+    if (!Tail || !ok || L < part) return kEmpty;
+    return __shfl_sync(g.mask, tail, lane_of_rank(g.mask, static_cast<int>((L - 1u) % n)));
   }
 
   __device__ static Group half_of(const Group& g, uint32_t pos, uint32_t first) {
@@ -895,7 +928,7 @@ struct VlStore {
       if (g.is_leader()) set_status(h, kErrCorrupt);
       return;
     }
-    if (b % kQcSpots == 0u) preallocate(h, q, g, c1, b);
+    if (b % kQcSpots == 0u) preallocate<PageQueue ? kPieceSegments : 1u>(h, q, g, c1, b);
     // A range may cover several queue chunks (a group that grew many chunks
     // of a small class): walk the chain one segment per queue chunk.
     uint32_t qc = c1;
@@ -906,7 +939,7 @@ struct VlStore {
         if (g.is_leader()) qc = next_of(h, qc);
         qc = bcast(g, qc);
         if (qc == kEmpty) break;
-        preallocate(h, q, g, qc, b + j0);   // b + j0 starts a queue chunk
+        preallocate<PageQueue ? kPieceSegments : 1u>(h, q, g, qc, b + j0);   // b + j0 starts a queue chunk
       }
       const uint32_t r2 = (j1 - j0 + n - 1u) / n;
       for (uint32_t i = 0; i < r2; ++i) {
@@ -941,7 +974,7 @@ struct VlStore {
     }
     if (qc == kEmpty) return;
     const uint32_t starts = __ballot_sync(sg.mask, pos % kQcSpots == 0u);
-    if (starts) preallocate(h, q, sg, qc, __shfl_sync(sg.mask, pos, __ffs(starts) - 1));
+    if (starts) preallocate<PageQueue ? kPieceSegments : 1u>(h, q, sg, qc, __shfl_sync(sg.mask, pos, __ffs(starts) - 1));
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), v);
     __syncwarp(sg.mask);
     __threadfence();
