@@ -254,11 +254,15 @@ struct VaStore {
     if (c < kInstalling) reuse_put(h, &h->reuse[0], c);
   }
 
-  // Count update of a range: m entries enqueued into the chunk of pos.
-  __device__ static void count_enqueued(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos, uint32_t m, bool recycle_ok) {
-    uint32_t add = (m << 16) + m;
-    uint32_t old = atomicAdd(&h->meta[c].qcount, add);
-    if (recycle_ok && old + add == kQcSpots) recycle(h, q, pos);
+  // Count update of a range: m entries enqueued into the chunk of pos (chunk
+  // queues: present << 16 | enqueued, which advance_front reads).  A page
+  // queue chunk is counted by its consumers alone -- every one of its 2048
+  // entries is taken exactly once, and only after it was written -- so its
+  // producers add nothing: the queue chunk's count line is not one more line
+  // that every group of a free burst passes through.
+  template <bool PageQueue>
+  __device__ static void count_enqueued(HeapCore* h, ClassState* q, uint32_t c, uint32_t pos, uint32_t m) {
+    if constexpr (!PageQueue) atomicAdd(&h->meta[c].qcount, (m << 16) + m);
   }
 
   // The lanes of a group hold contiguous positions that span at most two
@@ -299,9 +303,11 @@ struct VaStore {
           if (wait_slot_empty(h, s)) st_relaxed(s, value(j, cj));
         }
       }
-      __syncwarp(g.mask);
-      __threadfence();
-      if (g.is_leader()) count_enqueued(h, q, qc, b + j0, j1 - j0, PageQueue);
+      if constexpr (!PageQueue) {
+        __syncwarp(g.mask);
+        __threadfence();
+        if (g.is_leader()) count_enqueued<PageQueue>(h, q, qc, b + j0, j1 - j0);
+      }
     }
   }
 
@@ -318,9 +324,11 @@ struct VaStore {
       uint32_t* s = queue_slots(h, qc) + (pos % kQcSpots);
       if (wait_slot_empty(h, s)) st_relaxed(s, v);
     }
-    __syncwarp(sg.mask);
-    __threadfence();
-    if (sg.is_leader() && qc != kEmpty) count_enqueued(h, q, qc, pos, static_cast<uint32_t>(sg.size), PageQueue);
+    if constexpr (!PageQueue) {
+      __syncwarp(sg.mask);
+      __threadfence();
+      if (sg.is_leader() && qc != kEmpty) count_enqueued<PageQueue>(h, q, qc, pos, static_cast<uint32_t>(sg.size));
+    }
   }
 
   __device__ static uint32_t consume_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos) {
@@ -332,9 +340,10 @@ struct VaStore {
     if (qc != kEmpty) v = take_slot(h, queue_slots(h, qc) + (pos % kQcSpots));
     __syncwarp(sg.mask);
     if (sg.is_leader() && qc != kEmpty) {
-      uint32_t sub = static_cast<uint32_t>(sg.size) << 16;
-      uint32_t old = atomicSub(&h->meta[qc].qcount, sub);
-      if (old - sub == kQcSpots) recycle(h, q, pos);
+      // entries taken, in the upper half; the taker of the last one recycles
+      const uint32_t add = static_cast<uint32_t>(sg.size) << 16;
+      const uint32_t old = atomicAdd(&h->meta[qc].qcount, add);
+      if ((old + add) >> 16 == kQcSpots) recycle(h, q, pos);
     }
     return v;
   }
