@@ -48,6 +48,7 @@ GiB = 1 << 30
 SEED = 0x9E3779B9
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+REFERENCE_CELLS = os.path.join(ROOT, "profiles", "reference_cells.json")
 # Instantiations whose reference code faulted on the GPU on a cell of this
 # benchmark that its capacity model admits; the reference arm does not run
 # them again.
@@ -607,6 +608,26 @@ def config1_bench(arm_cls, stream, steps=10) -> dict:
             "null_results": nulls, "bad_words": bad, "flags": flags}
 
 
+def against_reference_cells(per_cell: dict, cold: dict) -> dict | None:
+    """Per-instantiation geometric-mean and smallest per-cell ratios of this
+    run's cells against a recorded reference-arm run (warm and cold); reported
+    beside the headline, which the driver compares with its own reference run."""
+    try:
+        ref = json.load(open(REFERENCE_CELLS))
+    except Exception:
+        return None
+    out = {}
+    for key, mine, theirs in (("warm", per_cell, ref["per_cell"]), ("cold", cold, ref["cold_per_cell"])):
+        by = {}
+        for cell, r in theirs.items():
+            if cell in mine and r["mops"] > 0:
+                by.setdefault(cell.split(":")[0], []).append(mine[cell]["mops"] / r["mops"])
+        out[key] = {v: {"geomean": round(float(np.exp(np.mean(np.log(x)))), 2), "min": round(min(x), 2)}
+                    for v, x in by.items()}
+    out["source"] = "profiles/reference_cells.json (" + ref.get("command", "") + ")"
+    return out
+
+
 def cpu_baseline(cells, n, heap_bytes) -> dict:
     """The oracle port (one host thread) over every cell, 2^20 requests each,
     one alloc pass and one free pass; plus glibc malloc/free on all host cores."""
@@ -1060,7 +1081,11 @@ def main():
     }
     if args.impl == "reference":
         out["cells_unavailable"] = skipped
-    elif value_ref_cells:
+    else:
+        vs = against_reference_cells(per_cell, out["cold"]["per_cell"])
+        if vs:
+            out["per_cell_vs_reference"] = vs
+    if args.impl != "reference" and value_ref_cells:
         out["value_on_reference_cells"] = {
             "value": round(value_ref_cells, 3), "unit": "Mops/s", "cells": len(ref_cells),
             "what": "the same aggregate over the cells the reference arm measures (all but "

@@ -502,10 +502,41 @@ __device__ void chunk_alloc_run(HeapCore* h, ClassState* q, const Group& s, type
       if (served && !was) chunk = c;
     }
   }
-  const uint32_t rf = last ? chunk_dequeue<Store>(h, q, v, pos, false, &cur) : 0u;
-  const uint32_t removed = __ballot_sync(s.mask, rf != 0u);
-  if (removed && s.is_leader()) atomicSub(&q->entries.v, __popc(removed));
-  if (__ballot_sync(s.mask, (rf & kDrainedQc) != 0u)) Store::after_drain(h, q, s);
+  // The takers of the chunks' last pages remove their entries together: each
+  // claims its entry (queue_pos) and writes the tombstone, then the removals
+  // are counted once per counter (segment or queue chunk) and once on the
+  // class's entry count.  A run's positions are consecutive, so its removals
+  // nearly always share one counter, which every group of the burst would
+  // otherwise hit once per removal.
+  uint32_t key = kEmpty;
+  bool mine = false;
+  if (last) {
+    uint32_t* qp = &h->meta[v].queue_pos;
+    uint32_t seen = atomicCAS(qp, pos, kEmpty);   // only an enqueue in flight (kPending) is waited for
+    for (uint32_t it = 0; seen == kPending && it < 4096u;) {
+      backoff(it);
+      seen = atomicCAS(qp, pos, kEmpty);
+    }
+    if (seen == pos) {
+      mine = true;
+      key = Store::remove_mark(h, q, pos, &cur);
+    }
+  }
+  const uint32_t removed = __ballot_sync(s.mask, mine);
+  uint32_t drained = 0;
+  if (removed) {
+    __syncwarp(s.mask);
+    __threadfence();   // tombstones before counts; queue_pos before the count re-check below
+    const uint32_t keyed = __ballot_sync(s.mask, mine && key != kEmpty);
+    if (mine && key != kEmpty) {
+      const Group kg = group_by(keyed, key);
+      if (kg.is_leader() && Store::remove_count(h, q, key, static_cast<uint32_t>(kg.size))) drained = 1u;
+    }
+    if (s.is_leader()) atomicSub(&q->entries.v, __popc(removed));
+    // a free that raced with the removal may have found the entry still there
+    if (mine && ld_relaxed(&h->meta[v].count) > 0) ensure_enqueued<Store>(h, q, v);
+  }
+  if (__ballot_sync(s.mask, drained != 0u)) Store::after_drain(h, q, s);
   if (removed) help_front<Store>(h, q, s);
 }
 

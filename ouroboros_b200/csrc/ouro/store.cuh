@@ -142,6 +142,18 @@ struct FlatStore {
     atomicAdd(seg_count(q, pos), 1u);
     return false;
   }
+  // remove() in two steps, so that a group counts its removals once per
+  // counter: remove_mark writes the tombstone and returns the key of the
+  // counter (the segment), remove_count (after a fence of every lane that
+  // marked) adds m removals to it.
+  __device__ static uint32_t remove_mark(HeapCore* h, ClassState* q, uint32_t pos, const Cursor* = nullptr) {
+    st_relaxed(slot(q, pos), kTomb);
+    return pos / 2048u;
+  }
+  __device__ static bool remove_count(HeapCore* h, ClassState* q, uint32_t key, uint32_t m) {
+    atomicAdd(q->seg + (key & q->seg_mask), m);
+    return false;
+  }
   __device__ static void after_drain(HeapCore*, ClassState*, const Group&) {}
 
   // Move the front past removed entries, freeing their slots for the next lap.
@@ -382,6 +394,18 @@ struct VaStore {
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
     atomicSub(&h->meta[qc].qcount, 1u << 16);
     return false;   // queue chunks return to the pool from the front
+  }
+  // remove() in two steps (see FlatStore): the key is the queue chunk.
+  __device__ static uint32_t remove_mark(HeapCore* h, ClassState* q, uint32_t pos, const Cursor* at = nullptr) {
+    uint32_t qc = at ? at->chunk : kEmpty;
+    if (qc == kEmpty) qc = ld_acquire(q->ring + vid(q, pos));
+    if (qc >= kInstalling) return kEmpty;
+    st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
+    return qc;
+  }
+  __device__ static bool remove_count(HeapCore* h, ClassState* q, uint32_t key, uint32_t m) {
+    atomicSub(&h->meta[key].qcount, m << 16);
+    return false;
   }
   __device__ static void after_drain(HeapCore*, ClassState*, const Group&) {}
   // Front moves over removed entries; passing the last entry of a queue chunk
@@ -841,7 +865,7 @@ struct VlStore {
   static constexpr uint32_t kPieceSegments = 4u;
   template <uint32_t Segments = 1u>
   __device__ static void preallocate(HeapCore* h, ClassState* q, const Group& g, uint32_t c, uint32_t pos) {
-    const uint32_t n = static_cast<uint32_t>(g.size), r = static_cast<uint32_t>(g.rank);
+    const uint32_t n = static_cast<uint32_t>(g.size);
     uint32_t ahead = 0;
     if (g.is_leader() && ld_relaxed(&h->meta[c].next) == kEmpty) {
       const uint32_t back = ld_relaxed(&q->back.v);
@@ -852,15 +876,15 @@ struct VlStore {
     ahead = bcast(g, ahead);
     if constexpr (Segments == 1u) {
       if (ahead) link_piece<false>(h, q, g, c, pos, ahead);
-      return;
-    }
-    while (ahead) {
-      const uint32_t part = ahead < kPieceRounds * n ? ahead : kPieceRounds * n;
-      const uint32_t last = link_piece<true>(h, q, g, c, pos, part);
-      if (last == kEmpty) return;   // a shorter piece, none, or someone else linked c
-      ahead -= part;
-      c = last;
-      pos += part * kQcSpots;
+    } else {
+      while (ahead) {
+        const uint32_t part = ahead < kPieceRounds * n ? ahead : kPieceRounds * n;
+        const uint32_t last = link_piece<true>(h, q, g, c, pos, part);
+        if (last == kEmpty) return;   // a shorter piece, none, or someone else linked c
+        ahead -= part;
+        c = last;
+        pos += part * kQcSpots;
+      }
     }
   }
 
@@ -1065,6 +1089,19 @@ struct VlStore {
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
     __threadfence();
     return count_removed(h, q, qc, 1u);
+  }
+  // remove() in two steps (see FlatStore): the key is the queue chunk;
+  // remove_count returns true when the m removals drained it.
+  __device__ static uint32_t remove_mark(HeapCore* h, ClassState* q, uint32_t pos, const Cursor* at = nullptr) {
+    uint32_t qc = at ? at->chunk : kEmpty;
+    if (qc == kEmpty || ld_relaxed(&h->meta[qc].vstart) / kQcSpots != pos / kQcSpots)
+      qc = locate_live(h, q, &q->front_ptr, pos);
+    if (qc == kEmpty || qc == kBehind) return kEmpty;
+    st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), kTomb);
+    return qc;
+  }
+  __device__ static bool remove_count(HeapCore* h, ClassState* q, uint32_t key, uint32_t m) {
+    return count_removed(h, q, key, m);
   }
   __device__ static void after_drain(HeapCore* h, ClassState* q, const Group& g) { on_empty(h, q, g); }
   // Front moves over removed entries.  The leader walks the chain: per round
