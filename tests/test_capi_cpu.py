@@ -44,3 +44,15 @@ def test_size_classes_match_oracle_encoding():
         inst, q = divmod(cls, 16)
         ps = (16 << q) if inst == 0 else (16384 << q)
         assert size <= ps and (size <= 16 if q == 0 and inst == 0 else size > ps // 2 or (inst == 1 and q == 0))
+
+
+def test_config_defaults_and_refusals_without_a_device():
+    # the defaults are the reference's compile-time parameters (include/Parameters.h:9-18)
+    c = ob.default_config().as_dict()
+    assert c == {"chunk_bytes": 8192, "page_queue_entries": 1 << 23, "virtual_queue_entries": 16384, "agg_width": 32}
+    out = ctypes.c_void_p()
+    for bad in ({"chunk_bytes": 4096}, {"page_queue_entries": 3 << 16}, {"page_queue_entries": 1 << 24},
+                {"virtual_queue_entries": 16}, {"agg_width": 3}, {"agg_width": 0}):
+        cfg = ob.default_config(**bad)
+        assert ob.lib().ouro_create_config(0, 1 << 30, ctypes.byref(cfg), ctypes.byref(out)) == 1, bad
+    assert ob.lib().ouro_config_default(None) == 1
