@@ -223,7 +223,12 @@ __device__ void chunk_enqueue(HeapCore* h, ClassState* q, uint32_t c) {
 // chunk_enqueue for the lanes of g, one chunk each, whose queue_pos the
 // lanes have already moved from kEmpty to kPending: one reservation of g.size
 // entries and back positions for the whole group instead of one per chunk.
-template <class Store>
+// Seg: pieces of queue chunks one link call of a linked queue may attach
+// (0: the default, one).  The frees of a burst re-enqueue up to one chunk per
+// lane, so a free launch may need many queue chunks in a row; the allocation
+// paths keep one, which keeps their kernels' code small.
+constexpr uint32_t kFreeEnqueueSegments = 4u;
+template <class Store, uint32_t Seg = 0u>
 __device__ void chunk_enqueue_group(HeapCore* h, ClassState* q, const Group& g, uint32_t c) {
   const uint32_t n = static_cast<uint32_t>(g.size);
   uint32_t b = 0, full = 0;
@@ -244,7 +249,7 @@ __device__ void chunk_enqueue_group(HeapCore* h, ClassState* q, const Group& g, 
   const uint32_t pos = bcast(g, b) + static_cast<uint32_t>(g.rank);
   st_relaxed(&h->meta[c].queue_pos, pos);
   __threadfence();   // queue_pos before the entry: a consumer that finds the entry can remove it
-  Store::template publish_lane<false>(h, q, g, pos, c);
+  Store::template publish_lane<false, Seg>(h, q, g, pos, c);
 }
 
 // A chunk whose count rose above zero must be findable: enqueue it unless it
@@ -798,7 +803,7 @@ __device__ void chunk_free(HeapCore* h, ClassState* q, const Group& g, uint32_t 
   }
   // the chunks of the warp that need an entry are enqueued together
   const uint32_t em = __ballot_sync(g.mask, enq != 0u);
-  if (enq) chunk_enqueue_group<Store>(h, q, make_group(em), c);
+  if (enq) chunk_enqueue_group<Store, kFreeEnqueueSegments>(h, q, make_group(em), c);
   flashed = __shfl_sync(cg.mask, flashed, cg.leader);
   help = __shfl_sync(cg.mask, help, cg.leader);
   if (__shfl_sync(cg.mask, drained, cg.leader)) Store::after_drain(h, q, cg);

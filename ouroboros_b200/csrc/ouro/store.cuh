@@ -108,7 +108,7 @@ struct FlatStore {
     }
   }
 
-  template <bool PageQueue = true>
+  template <bool PageQueue = true, uint32_t Seg = 0u>
   __device__ static void publish_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos, uint32_t v) {
     uint32_t* s = slot(q, pos);
     if (wait_slot_empty(h, s)) st_relaxed(s, v);
@@ -325,7 +325,7 @@ struct VaStore {
 
   // PageQueue false: a chunk queue, whose queue chunks return to the pool
   // from the front (advance_front), not when their entries are consumed.
-  template <bool PageQueue = true>
+  template <bool PageQueue = true, uint32_t Seg = 0u>
   __device__ static void publish_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos, uint32_t v) {
     const Group sg = half_of(g, pos, bcast(g, pos));
     if (pos % kQcSpots == 0u) preallocate(h, q, pos);
@@ -989,7 +989,8 @@ struct VlStore {
     }
   }
 
-  template <bool PageQueue = true>
+  // Seg: pieces one preallocate call may link (0: the queue kind's default).
+  template <bool PageQueue = true, uint32_t Seg = 0u>
   __device__ static void publish_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos, uint32_t v) {
     const uint32_t first = bcast(g, pos);
     uint32_t c1 = kEmpty;
@@ -1007,7 +1008,8 @@ struct VlStore {
     }
     if (qc == kEmpty) return;
     const uint32_t starts = __ballot_sync(sg.mask, pos % kQcSpots == 0u);
-    if (starts) preallocate<PageQueue ? kPieceSegments : 1u>(h, q, sg, qc, __shfl_sync(sg.mask, pos, __ffs(starts) - 1));
+    if (starts)
+      preallocate<Seg ? Seg : (PageQueue ? kPieceSegments : 1u)>(h, q, sg, qc, __shfl_sync(sg.mask, pos, __ffs(starts) - 1));
     st_relaxed(queue_slots(h, qc) + (pos % kQcSpots), v);
     __syncwarp(sg.mask);
     __threadfence();
