@@ -381,9 +381,13 @@ struct VaStore {
     uint32_t qc = ld_acquire(q->ring + vid(q, pos));
     cur.chunk = kEmpty;
     if (qc >= kInstalling) return kEmpty;
-    if (ld_relaxed(&h->meta[qc].vstart) / kQcSpots != pos / kQcSpots) return kTomb;
+    // the queue chunk's range and the entry are read together; an entry of a
+    // queue chunk that holds another range is discarded
+    const uint32_t vs = ld_relaxed(&h->meta[qc].vstart);
+    const uint32_t v = ld_acquire(queue_slots(h, qc) + (pos % kQcSpots));
+    if (vs / kQcSpots != pos / kQcSpots) return kTomb;
     cur.chunk = qc;
-    return ld_acquire(queue_slots(h, qc) + (pos % kQcSpots));
+    return v;
   }
   // at: the cursor of the peek that found pos's entry, which the caller is
   // removing; its queue chunk cannot drain or be reused before this removal.
@@ -502,10 +506,11 @@ struct VlStore {
   }
   __device__ static uint32_t recall_range(HeapCore* h, ClassState* q, uint32_t range) {
     const uint32_t c = ld_relaxed(q->skip + (range & (kSkipSlots - 1u)));
-    if (c < h->max_chunks && ld_relaxed(&h->meta[c].size) == queue_tag(q) &&
-        ld_relaxed(&h->meta[c].vstart) / kQcSpots == range)
-      return c;
-    return kEmpty;
+    if (c >= h->max_chunks) return kEmpty;
+    // tag and range are read together (two loads in flight, not one after the other)
+    const uint32_t tag = ld_relaxed(&h->meta[c].size);
+    const uint32_t vs = ld_relaxed(&h->meta[c].vstart);
+    return (tag == queue_tag(q) && vs / kQcSpots == range) ? c : kEmpty;
   }
   __device__ static uint32_t recall(HeapCore* h, ClassState* q, uint32_t pos) {
     return recall_range(h, q, pos / kQcSpots);
