@@ -237,8 +237,9 @@ struct VaStore {
 
   __device__ static uint32_t vid(const ClassState* q, uint32_t pos) { return (pos / kQcSpots) & q->ring_mask; }
 
-  // The queue chunk holding pos (spins while its pre-allocation is in flight).
-  __device__ static uint32_t qchunk(HeapCore* h, ClassState* q, uint32_t pos) {
+  // The index entry of pos's range (spins while its pre-allocation is in
+  // flight), not yet checked against the queue chunk's range.
+  __device__ static uint32_t qchunk_entry(HeapCore* h, ClassState* q, uint32_t pos) {
     uint32_t* e = q->ring + vid(q, pos);
     uint32_t c, it = 0;
     while ((c = ld_acquire(e)) == kEmpty || c == kInstalling) {
@@ -247,11 +248,29 @@ struct VaStore {
         install_queue_chunk(h, e, q->inst, pos - pos % kQcSpots, queue_tag(q));
       backoff(it);
     }
+    return c;
+  }
+  // The queue chunk holding pos, checked.
+  __device__ static uint32_t qchunk(HeapCore* h, ClassState* q, uint32_t pos) {
+    const uint32_t c = qchunk_entry(h, q, pos);
+    if (c == kEmpty) return kEmpty;
     if (ld_relaxed(&h->meta[c].vstart) / kQcSpots != pos / kQcSpots) {
       set_status(h, kErrCorrupt);
       return kEmpty;
     }
     return c;
+  }
+  // The half group sg holds positions of one range; its leader found the
+  // entry qc.  The check of qc's range and every lane's first look at its
+  // slot go out together; false (and the corruption flag) on a mismatch.
+  __device__ static bool range_ok(HeapCore* h, const Group& sg, uint32_t qc, uint32_t pos, uint32_t* s,
+                                  uint32_t* first, bool acquire) {
+    uint32_t vs = 0;
+    if (sg.is_leader()) vs = ld_relaxed(&h->meta[qc].vstart);
+    *first = acquire ? ld_acquire(s) : ld_relaxed(s);
+    const bool ok = bcast(sg, vs / kQcSpots == pos / kQcSpots ? 1u : 0u) != 0u;
+    if (!ok && sg.is_leader()) set_status(h, kErrCorrupt);
+    return ok;
   }
 
   // The producer of a position at the start of a queue chunk allocates the
@@ -330,11 +349,13 @@ struct VaStore {
     const Group sg = half_of(g, pos, bcast(g, pos));
     if (pos % kQcSpots == 0u) preallocate(h, q, pos);
     uint32_t qc = kEmpty;
-    if (sg.is_leader()) qc = qchunk(h, q, pos);
+    if (sg.is_leader()) qc = qchunk_entry(h, q, pos);
     qc = bcast(sg, qc);
     if (qc != kEmpty) {
       uint32_t* s = queue_slots(h, qc) + (pos % kQcSpots);
-      if (wait_slot_empty(h, s)) st_relaxed(s, v);
+      uint32_t first = 0;
+      if (!range_ok(h, sg, qc, pos, s, &first, false)) qc = kEmpty;
+      else if (first == kEmpty || wait_slot_empty(h, s)) st_relaxed(s, v);
     }
     if constexpr (!PageQueue) {
       __syncwarp(sg.mask);
@@ -346,10 +367,21 @@ struct VaStore {
   __device__ static uint32_t consume_lane(HeapCore* h, ClassState* q, const Group& g, uint32_t pos) {
     const Group sg = half_of(g, pos, bcast(g, pos));
     uint32_t qc = kEmpty;
-    if (sg.is_leader()) qc = qchunk(h, q, pos);
+    if (sg.is_leader()) qc = qchunk_entry(h, q, pos);
     qc = bcast(sg, qc);
     uint32_t v = kEmpty;
-    if (qc != kEmpty) v = take_slot(h, queue_slots(h, qc) + (pos % kQcSpots));
+    if (qc != kEmpty) {
+      uint32_t* s = queue_slots(h, qc) + (pos % kQcSpots);
+      uint32_t first = kEmpty;
+      if (!range_ok(h, sg, qc, pos, s, &first, true)) {
+        qc = kEmpty;
+      } else if (first != kEmpty) {
+        st_relaxed(s, kEmpty);   // take_slot's first poll found it
+        v = first;
+      } else {
+        v = take_slot(h, s);
+      }
+    }
     __syncwarp(sg.mask);
     if (sg.is_leader() && qc != kEmpty) {
       // entries taken, in the upper half; the taker of the last one recycles
