@@ -314,15 +314,21 @@ __device__ uint32_t chunk_dequeue(HeapCore* h, ClassState* q, uint32_t c, uint32
 // one word at a time and stopping as soon as enough bits are won: it picks
 // the lowest set bits in rotated order, clears them with one atomicAnd, and
 // the group hands the won bits to its unserved lanes by rank.
+// `words`: the mask words the search visits.  A lone lane visits all W, in
+// the reference's order (sequential parity); a group of two or more visits
+// only the words the class's pages occupy (ceil(pages per chunk / 32)), since
+// the rest are always empty: starting at (tid + 1) mod 16, a 256 B group
+// otherwise loaded up to 15 empty words one after another before its own.
 template <uint32_t W>
-__device__ void claim_pages(HeapCore* h, const Group& s, uint32_t c, uint32_t got, bool& served, uint32_t& page) {
+__device__ void claim_pages(HeapCore* h, const Group& s, uint32_t c, uint32_t got, bool& served, uint32_t& page,
+                            uint32_t words = W) {
   ChunkMeta* m = h->meta + c;
-  const uint32_t start = bcast(s, (threadIdx.x + 1u) % W);
+  const uint32_t start = bcast(s, (threadIdx.x + 1u) % words);
   const uint32_t offset = bcast(s, (threadIdx.x + blockIdx.x) % 32u);
   uint32_t remaining = got;
   for (uint32_t attempt = 0; attempt < 64u && remaining; ++attempt) {
-    for (uint32_t j = 0; j < W && remaining; ++j) {
-      const uint32_t w = (start + j) % W;
+    for (uint32_t j = 0; j < words && remaining; ++j) {
+      const uint32_t w = (start + j) % words;
       uint32_t won = 0;
       if (s.is_leader()) {
         const uint32_t rot = rotr32(ld_relaxed(m->mask(w)), offset);
@@ -502,7 +508,7 @@ __device__ void chunk_alloc_run(HeapCore* h, ClassState* q, const Group& s, type
       const uint32_t c = __shfl_sync(s.mask, v, src);
       const uint32_t k = __shfl_sync(s.mask, got, src);
       const bool was = served;
-      if (q->inst == 0u) claim_pages<16u>(h, s, c, k, served, page);
+      if (q->inst == 0u) claim_pages<16u>(h, s, c, k, served, page, (q->ppc + 31u) / 32u);
       else claim_pages<1u>(h, s, c, k, served, page);
       if (served && !was) chunk = c;
     }
@@ -658,7 +664,7 @@ __device__ void* chunk_alloc(HeapCore* h, ClassState* q, const Group& g) {
 #ifdef OURO_SCAN_STATS
       long long t0 = clock64();
 #endif
-      if (q->inst == 0u) claim_pages<16u>(h, s, c, got, served, page);
+      if (q->inst == 0u) claim_pages<16u>(h, s, c, got, served, page, s.size > 1 ? (q->ppc + 31u) / 32u : 16u);
       else claim_pages<1u>(h, s, c, got, served, page);
 #ifdef OURO_SCAN_STATS
       t_claim += clock64() - t0;
