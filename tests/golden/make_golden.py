@@ -2,9 +2,10 @@
 
 For every variant and every trace of traces.py, the reference allocator itself
 (oracle/_ref/libouro_ref.so, the reference's headers compiled for sm_100a by
-oracle/Makefile) replays the trace with one GPU thread on a fresh 1 GiB heap.
-The byte offsets it returns (page address minus the reference's d_data) and its
-counters after the trace are written to trace_<variant>.npz.  The reference has
+oracle/Makefile) replays the trace with one GPU thread on a fresh heap (1 GiB unless
+traces.HEAPS names another size).  The byte offsets it returns (page address
+minus the reference's d_data; for the traces of traces.DIGEST_ONLY their
+SHA-256) and its counters after the trace are written to trace_<variant>.npz.  The reference has
 no tests or known-answer vectors of its own; these fixtures are its outputs.
 
     python tests/golden/make_golden.py <out_dir> [trace names]
@@ -32,6 +33,16 @@ def ops_digest(ops: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(ops, dtype=np.uint32).tobytes()).hexdigest()
 
 
+# The reference's VAC code faulted here under concurrency (an illegal memory
+# access in the 1024 B cell of the 2^20-thread benchmark); it is not run on
+# workloads it has not already completed.
+NOT_RUN = {("VAC", "large4g")}
+
+
+def offsets_digest(off: np.ndarray) -> bytes:
+    return hashlib.sha256(np.ascontiguousarray(off, dtype=np.int64).tobytes()).digest()
+
+
 def main(out_dir: str, names=None) -> int:
     os.makedirs(out_dir, exist_ok=True)
     built = {name: traces.build(name) for name in (names or traces.TRACES)}
@@ -41,13 +52,19 @@ def main(out_dir: str, names=None) -> int:
         if names and os.path.exists(path):
             arrays.update(np.load(path))
         for name, (ops, tid, bid) in built.items():
-            ref = oracle.RefDriver(v, traces.HEAP_BYTES)
-            if "init_state" not in arrays:
+            if (v, name) in NOT_RUN:
+                continue
+            heap = traces.heap_bytes(name)
+            ref = oracle.RefDriver(v, heap)
+            if "init_state" not in arrays and heap == traces.HEAP_BYTES:
                 arrays["init_state"] = ref.state()
                 info = ref.info()
                 arrays["meta"] = np.array([info["max_chunks"], info["allocation_bytes"]], dtype=np.uint64)
             off = ref.run_trace(ops, tid, bid)
-            arrays[f"{name}_off"] = off
+            if name in traces.DIGEST_ONLY:
+                arrays[f"{name}_off_sha256"] = np.frombuffer(offsets_digest(off), dtype=np.uint8)
+            else:
+                arrays[f"{name}_off"] = off
             arrays[f"{name}_state"] = ref.state()
             arrays[f"{name}_ops_sha256"] = np.frombuffer(bytes.fromhex(ops_digest(ops)), dtype=np.uint8)
             ref.close()

@@ -48,6 +48,16 @@ class _Builder:
         for i in list(self.live if order is None else order):
             self.free(i)
 
+    def free_many(self, ids):
+        """free(i) for every i of ids, in that order, with one pass over the
+        live list (free() searches it once per call)."""
+        ids = [int(i) for i in ids]
+        for i in ids:
+            self.ops += [1, i]
+        gone = set(ids)
+        assert len(gone) == len(ids) and gone <= set(self.live)
+        self.live = [i for i in self.live if i not in gone]
+
     def array(self) -> np.ndarray:
         return np.asarray(self.ops, dtype=np.uint32)
 
@@ -162,6 +172,27 @@ def initial() -> np.ndarray:
     return b.array()
 
 
+def large(seed: int = 3) -> np.ndarray:
+    """At scale, on a 4 GiB heap: 2^15 requests of 2 KiB, 2^16 of 64 B and
+    2^14 of 8 KiB (about 25,000 chunks; the 64 B page queue passes through 32
+    queue chunks), then a third of the small requests and all the 8 KiB ones
+    freed in a random order (chunk-based queues re-enqueue partly used chunks
+    and return the emptied ones to the reuse queue), 2^15 re-allocations of
+    64 B .. 8 KiB that take those pages and chunks again, and everything freed
+    in the reverse order of allocation."""
+    rng = np.random.default_rng(seed)
+    b = _Builder()
+    k2 = [b.malloc(2048) for _ in range(1 << 15)]
+    s64 = [b.malloc(64) for _ in range(1 << 16)]
+    k8 = [b.malloc(8192) for _ in range(1 << 14)]
+    victims = np.asarray(k2[::3] + s64[1::3] + k8)
+    b.free_many(victims[rng.permutation(victims.size)])
+    for size in rng.choice(np.asarray([64, 1024, 2048, 8192]), size=1 << 15):
+        b.malloc(int(size))
+    b.free_many(b.live[::-1])
+    return b.array()
+
+
 # name -> (builder, tid, bid): the GPU thread that replays the trace
 TRACES = {
     "basic": (basic, 0, 0),
@@ -172,7 +203,19 @@ TRACES = {
     "chunk_fifo": (chunk_fifo, 0, 0),
     "tier2": (tier2, 0, 0),
     "initial": (initial, 0, 0),
+    "large4g": (large, 0, 0),
 }
+
+# traces replayed on a heap other than HEAP_BYTES
+HEAPS = {"large4g": 4 << 30}
+
+# traces whose reference offsets are pinned by their SHA-256 instead of being
+# stored whole (the fixture would hold about 200,000 of them per variant)
+DIGEST_ONLY = {"large4g"}
+
+
+def heap_bytes(name: str) -> int:
+    return HEAPS.get(name, HEAP_BYTES)
 
 
 def build(name: str):

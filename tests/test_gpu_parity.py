@@ -35,11 +35,11 @@ def test_init_state_matches_oracle(v):
 @pytest.mark.parametrize("v", ob.VARIANTS)
 def test_trace_matches_oracle(v, name):
     ops, tid, bid = traces.build(name)
-    with ob.Ouroboros(v, traces.HEAP_BYTES) as heap:
+    with ob.Ouroboros(v, traces.heap_bytes(name)) as heap:
         got = heap.trace(ops, tid, bid)
         st = heap.state()
         flags = heap.status()["flags"]
-    o = oracle.Oracle(v, traces.HEAP_BYTES, tid, bid)
+    o = oracle.Oracle(v, traces.heap_bytes(name), tid, bid)
     want, _ = o.run_trace(ops)
     assert flags == 0
     bad = np.nonzero(got != want)[0]

@@ -2,7 +2,8 @@
 
 tests/golden/trace_<variant>.npz hold what the reference allocator, compiled for
 sm_100a, returned when one GPU thread replayed each trace of traces.py on a
-fresh 1 GiB heap (generator: tests/golden/make_golden.py).  The oracle must
+fresh heap of 1 GiB (4 GiB for the large trace; generator:
+tests/golden/make_golden.py).  The oracle must
 reproduce every byte offset and every counter bit-exactly.
 """
 import os
@@ -12,7 +13,7 @@ import pytest
 
 import oracle
 from tests.golden import traces
-from tests.golden.make_golden import ops_digest
+from tests.golden.make_golden import NOT_RUN, offsets_digest, ops_digest
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -34,14 +35,19 @@ def test_layout_and_init_state(v):
 @pytest.mark.parametrize("name", list(traces.TRACES))
 @pytest.mark.parametrize("v", oracle.VARIANTS)
 def test_trace_bit_exact(v, name):
+    if (v, name) in NOT_RUN:
+        pytest.skip("the reference's VAC code is not run at this scale (it faulted under concurrency)")
     g = _golden(v)
     ops, tid, bid = traces.build(name)
     assert bytes(g[f"{name}_ops_sha256"]).hex() == ops_digest(ops), "trace generator drifted from the fixture"
-    o = oracle.Oracle(v, traces.HEAP_BYTES, tid, bid)
+    o = oracle.Oracle(v, traces.heap_bytes(name), tid, bid)
     res, off = o.run_trace(ops)
-    gold = g[f"{name}_off"]
-    bad = np.nonzero(off != gold)[0]
-    assert bad.size == 0, f"first mismatch at op {bad[0]}: oracle {off[bad[0]]} reference {gold[bad[0]]}"
+    if name in traces.DIGEST_ONLY:
+        assert offsets_digest(off) == bytes(g[f"{name}_off_sha256"]), "offsets differ from the reference's"
+    else:
+        gold = g[f"{name}_off"]
+        bad = np.nonzero(off != gold)[0]
+        assert bad.size == 0, f"first mismatch at op {bad[0]}: oracle {off[bad[0]]} reference {gold[bad[0]]}"
     st = o.state()
     sbad = np.nonzero(st != g[f"{name}_state"])[0]
     assert sbad.size == 0, f"state words differ: {sbad.tolist()}"
