@@ -121,6 +121,28 @@ int ouro_alloc(ouro_heap* h, uint32_t n, uint32_t size, const uint32_t* d_sizes,
 /* src/main.cu:55-63 d_testFree: thread i frees d_ptrs[i] (nullptr is a no-op). */
 int ouro_free(ouro_heap* h, uint32_t n, void* const* d_ptrs, int block, void* stream);
 
+/* ouro_alloc / ouro_free for requests held in HOST memory (no counterpart in
+ * the reference, whose callers are device code: this is the entry point for a
+ * host-side caller).  ouro_alloc_host: request i is malloc(size), or
+ * malloc(h_sizes[i]) when h_sizes is not NULL; its pointer goes to h_out[i]
+ * and, when d_out is not NULL, to d_out[i] (device) too.  ouro_free_host:
+ * frees h_ptrs[i].  The requests are cut into `slices` pieces (0: 1 to 4 by
+ * n, at least 2^17 requests each; at most 8) whose host<->device copies, on
+ * two streams of the heap's own, overlap the launches of the other pieces.
+ * The work is ordered after what `stream` holds at the call and after the
+ * previous host-buffer call on this heap, and it ends on `stream`:
+ * synchronise `stream` before reading h_out or reusing the host buffers.
+ * Pinned host memory makes the copies asynchronous; pageable memory works,
+ * with copies that do not overlap.  Calls on one heap from several host
+ * threads take turns. */
+int ouro_alloc_host(ouro_heap* h, uint32_t n, uint32_t size, const uint32_t* h_sizes, void** h_out, void** d_out,
+                    int block, int slices, void* stream);
+int ouro_free_host(ouro_heap* h, uint32_t n, void* const* h_ptrs, int block, int slices, void* stream);
+/* Makes the host-buffer calls' streams, events and device staging for batches
+ * of up to n requests now, so that no later call of up to n requests creates
+ * them (the first call on a heap otherwise does, synchronously). */
+int ouro_host_reserve(ouro_heap* h, uint32_t n);
+
 /* Sequential replay of an op trace by one GPU thread (threadIdx.x = tid,
  * blockIdx.x = bid) for parity with the reference.  Op kinds, ops[2i] with
  * argument a = ops[2i+1]:

@@ -44,6 +44,7 @@ EXPORTS = (
     "ouro_allocate_chunk", "ouro_enqueue_initial_chunk", "ouro_batch_reserve",
     "ouro_serve_start", "ouro_serve_submit", "ouro_serve_poll", "ouro_serve_stop", "ouro_serve_close",
     "ouro_config_default", "ouro_create_config", "ouro_get_config", "ouro_autotune_config",
+    "ouro_alloc_host", "ouro_free_host", "ouro_host_reserve",
 )
 
 
@@ -168,6 +169,9 @@ def lib():
         L.ouro_get_info.argtypes = [p, ctypes.POINTER(_Info)]
         L.ouro_alloc.argtypes = [p, u32, u32, p, p, i, p]
         L.ouro_free.argtypes = [p, u32, p, i, p]
+        L.ouro_alloc_host.argtypes = [p, u32, u32, p, p, p, i, i, p]
+        L.ouro_free_host.argtypes = [p, u32, p, i, i, p]
+        L.ouro_host_reserve.argtypes = [p, u32]
         L.ouro_trace.argtypes = [p, p, u64, p, u32, u32]
         L.ouro_state.argtypes = [p, p]
         L.ouro_get_status.argtypes = [p, ctypes.POINTER(_Status), i]
@@ -209,11 +213,13 @@ def _check(rc: int, what: str):
 
 
 def _addr(x) -> int | None:
-    """Device address of a tensor / int / None."""
+    """Address of a tensor (device or host), a numpy array, an int, or None."""
     if x is None:
         return None
     if isinstance(x, int):
         return x or None
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data or None
     return x.data_ptr()
 
 
@@ -290,6 +296,24 @@ class Ouroboros:
 
     def free(self, ptrs, n: int, block: int = 256, stream=None):
         _check(lib().ouro_free(self._handle(), n, _addr(ptrs), block, _stream(stream)), "ouro_free")
+
+    def alloc_host(self, out_host, n: int, size: int = 0, sizes_host=None, out_device=None, block: int = 256,
+                   slices: int = 0, stream=None):
+        """alloc() for requests and results in host memory (pinned for
+        overlapped copies): out_host[i] = malloc(size or sizes_host[i]), and
+        out_device[i] too when given.  Asynchronous on `stream`."""
+        _check(lib().ouro_alloc_host(self._handle(), n, size, _addr(sizes_host), _addr(out_host), _addr(out_device),
+                                     block, slices, _stream(stream)), "ouro_alloc_host")
+
+    def host_reserve(self, n: int):
+        """Streams, events and device staging of the host-buffer calls for up
+        to n requests, made now rather than by the first call."""
+        _check(lib().ouro_host_reserve(self._handle(), n), "ouro_host_reserve")
+
+    def free_host(self, ptrs_host, n: int, block: int = 256, slices: int = 0, stream=None):
+        """free() of a host-memory pointer array.  Asynchronous on `stream`."""
+        _check(lib().ouro_free_host(self._handle(), n, _addr(ptrs_host), block, slices, _stream(stream)),
+               "ouro_free_host")
 
     def allocate_chunk(self) -> int:
         """allocateChunk<false> of the first instance (Ouroboros.cuh:108-136): an

@@ -422,8 +422,11 @@ int ouro_create_config(int variant, uint64_t heap_bytes, const ouro_config* cfg_
   return OURO_OK;
 }
 
+static void host_release(ouro_heap* h);
+
 int ouro_destroy(ouro_heap* h) {
   if (!h) return OURO_ERR_ARG;
+  host_release(h);
   if (h->batch_scratch) cudaFree(h->batch_scratch);
   cudaError_t e = cudaFree(h->raw);
   delete h;
@@ -464,6 +467,157 @@ int ouro_free(ouro_heap* h, uint32_t n, void* const* d_ptrs, int block, void* st
         reinterpret_cast<Ouroboros<V>*>(h->dev), n, d_ptrs);
     return cuda_rc(cudaGetLastError());
   });
+}
+
+// ------------------------------------------------------------ host buffers
+// Requests and results in host memory.  The n requests are cut into slices:
+// a slice's request sizes (or pointers) go host->device on host_in, its launch
+// runs on the caller's stream once they are there, and (alloc) its pointers
+// come back device->host on host_out once the launch is done, so the copies of
+// one slice overlap the launches of the others.  Everything is ordered after
+// the work queued on `stream` before the call, and after the previous
+// host-buffer call on this heap (they share the staging), and it ends on
+// `stream`: the caller synchronises `stream` before reading the results.
+namespace {
+
+constexpr uint32_t kHostSlicesMax = 8u;
+constexpr uint32_t kHostSliceMin = 1u << 17;   // fewer requests per launch fill the GPU poorly
+
+uint32_t host_slices(uint32_t n, int slices) {
+  if (slices > 0) return n < static_cast<uint32_t>(slices) ? n : static_cast<uint32_t>(slices);
+  const uint32_t k = n / kHostSliceMin;
+  return k < 1u ? 1u : k > 4u ? 4u : k;
+}
+
+int host_prepare(ouro_heap* h, size_t bytes) {
+  if (!h->host_ready) {
+    bool ok = cudaStreamCreateWithFlags(&h->host_in, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&h->host_out, cudaStreamNonBlocking) == cudaSuccess;
+    cudaEvent_t* evs[3] = {&h->host_entry, &h->host_done, &h->host_joined};
+    for (cudaEvent_t* e : evs) ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+    for (uint32_t k = 0; k < kHostSlicesMax; ++k)
+      ok = ok && cudaEventCreateWithFlags(&h->host_slice_in[k], cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&h->host_slice_run[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+      (void)cudaGetLastError();
+      return OURO_ERR_CUDA;
+    }
+    h->host_ready = true;
+  }
+  if (h->host_stage_bytes < bytes) {
+    // cudaFree waits for the work still reading the old staging
+    if (h->host_stage) cudaFree(h->host_stage);
+    h->host_stage = nullptr;
+    h->host_stage_bytes = 0;
+    if (cudaMalloc(&h->host_stage, bytes) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return OURO_ERR_NOMEM;
+    }
+    h->host_stage_bytes = bytes;
+  }
+  return OURO_OK;
+}
+
+// The helper streams start after the caller's queued work and after the
+// previous host-buffer call's copies.
+void host_enter(ouro_heap* h, cudaStream_t s) {
+  cudaEventRecord(h->host_entry, s);
+  cudaStreamWaitEvent(h->host_in, h->host_entry, 0);
+  cudaStreamWaitEvent(h->host_in, h->host_done, 0);
+  cudaStreamWaitEvent(h->host_out, h->host_entry, 0);
+  cudaStreamWaitEvent(h->host_out, h->host_done, 0);
+}
+
+}  // namespace
+
+static void host_release(ouro_heap* h) {
+  if (h->host_ready) {
+    cudaStreamSynchronize(h->host_in);
+    cudaStreamSynchronize(h->host_out);
+    cudaStreamDestroy(h->host_in);
+    cudaStreamDestroy(h->host_out);
+    cudaEventDestroy(h->host_entry);
+    cudaEventDestroy(h->host_done);
+    cudaEventDestroy(h->host_joined);
+    for (uint32_t k = 0; k < kHostSlicesMax; ++k) {
+      cudaEventDestroy(h->host_slice_in[k]);
+      cudaEventDestroy(h->host_slice_run[k]);
+    }
+    h->host_ready = false;
+  }
+  if (h->host_stage) cudaFree(h->host_stage);
+  h->host_stage = nullptr;
+  h->host_stage_bytes = 0;
+}
+
+int ouro_host_reserve(ouro_heap* h, uint32_t n) {
+  if (!h) return OURO_ERR_ARG;
+  std::lock_guard<std::mutex> lock(h->host_mu);
+  // enough for ouro_alloc_host with per-request sizes and staged pointers
+  return host_prepare(h, ((4ull * n + 255u) & ~size_t(255)) + 8ull * n);
+}
+
+int ouro_alloc_host(ouro_heap* h, uint32_t n, uint32_t size, const uint32_t* h_sizes, void** h_out, void** d_out,
+                    int block, int slices, void* stream) {
+  if (!h || !h_out || block <= 0 || block > 1024 || slices < 0 || slices > static_cast<int>(kHostSlicesMax))
+    return OURO_ERR_ARG;
+  if (n == 0) return OURO_OK;
+  std::lock_guard<std::mutex> lock(h->host_mu);
+  const size_t sizes_bytes = h_sizes ? (4ull * n + 255u) & ~size_t(255) : 0u;
+  int rc = host_prepare(h, sizes_bytes + (d_out ? 0u : 8ull * n));
+  if (rc) return rc;
+  uint32_t* d_sizes = h_sizes ? static_cast<uint32_t*>(h->host_stage) : nullptr;
+  void** d_ptrs = d_out ? d_out : reinterpret_cast<void**>(static_cast<char*>(h->host_stage) + sizes_bytes);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const uint32_t k = host_slices(n, slices), m = (n + k - 1u) / k;
+  host_enter(h, s);
+  rc = dispatch(h->variant, [&](auto v) {
+    constexpr int V = decltype(v)::value;
+    for (uint32_t j = 0; j < k; ++j) {
+      const uint32_t o = j * m, c = n - o < m ? n - o : m;
+      if (h_sizes) {
+        cudaMemcpyAsync(d_sizes + o, h_sizes + o, 4ull * c, cudaMemcpyHostToDevice, h->host_in);
+        cudaEventRecord(h->host_slice_in[j], h->host_in);
+        cudaStreamWaitEvent(s, h->host_slice_in[j], 0);
+      }
+      k_alloc<V><<<grid_for(c, block), block, 0, s>>>(reinterpret_cast<Ouroboros<V>*>(h->dev), c, size,
+                                                         h_sizes ? d_sizes + o : nullptr, d_ptrs + o);
+      cudaEventRecord(h->host_slice_run[j], s);
+      cudaStreamWaitEvent(h->host_out, h->host_slice_run[j], 0);
+      cudaMemcpyAsync(h_out + o, d_ptrs + o, 8ull * c, cudaMemcpyDeviceToHost, h->host_out);
+    }
+    return OURO_OK;
+  });
+  cudaEventRecord(h->host_joined, h->host_out);
+  cudaStreamWaitEvent(s, h->host_joined, 0);   // host_in's copies all precede launches on s
+  cudaEventRecord(h->host_done, s);
+  return rc ? rc : cuda_rc(cudaGetLastError());
+}
+
+int ouro_free_host(ouro_heap* h, uint32_t n, void* const* h_ptrs, int block, int slices, void* stream) {
+  if (!h || !h_ptrs || block <= 0 || block > 1024 || slices < 0 || slices > static_cast<int>(kHostSlicesMax))
+    return OURO_ERR_ARG;
+  if (n == 0) return OURO_OK;
+  std::lock_guard<std::mutex> lock(h->host_mu);
+  int rc = host_prepare(h, 8ull * n);
+  if (rc) return rc;
+  void** d_ptrs = static_cast<void**>(h->host_stage);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const uint32_t k = host_slices(n, slices), m = (n + k - 1u) / k;
+  host_enter(h, s);
+  rc = dispatch(h->variant, [&](auto v) {
+    constexpr int V = decltype(v)::value;
+    for (uint32_t j = 0; j < k; ++j) {
+      const uint32_t o = j * m, c = n - o < m ? n - o : m;
+      cudaMemcpyAsync(d_ptrs + o, h_ptrs + o, 8ull * c, cudaMemcpyHostToDevice, h->host_in);
+      cudaEventRecord(h->host_slice_in[j], h->host_in);
+      cudaStreamWaitEvent(s, h->host_slice_in[j], 0);
+      k_free<V><<<grid_for(c, block), block, 0, s>>>(reinterpret_cast<Ouroboros<V>*>(h->dev), c, d_ptrs + o);
+    }
+    return OURO_OK;
+  });
+  cudaEventRecord(h->host_done, s);
+  return rc ? rc : cuda_rc(cudaGetLastError());
 }
 
 int ouro_trace(ouro_heap* h, const uint32_t* ops, uint64_t n_ops, uint64_t* results, uint32_t tid, uint32_t bid) {

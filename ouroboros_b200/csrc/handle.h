@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <type_traits>
 
 #include "../../include/ouroboros_b200.h"
@@ -22,6 +23,16 @@ struct ouro_heap {
   int batch_per_sm;   // kept for the C ABI's report; the serving launch is not persistent
   void* batch_scratch;              // batched path: sort counters and permutation (grown on demand)
   size_t batch_scratch_bytes;
+  // host-buffer entry points (ouro_alloc_host / ouro_free_host): device
+  // staging for request sizes and pointers, two copy streams and their
+  // events, made on first use; calls on one heap take turns on the mutex
+  void* host_stage;
+  size_t host_stage_bytes;
+  cudaStream_t host_in, host_out;
+  cudaEvent_t host_entry, host_done, host_joined;
+  cudaEvent_t host_slice_in[8], host_slice_run[8];
+  bool host_ready;
+  std::mutex host_mu;
 };
 
 namespace ouro {
