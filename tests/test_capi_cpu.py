@@ -56,3 +56,13 @@ def test_config_defaults_and_refusals_without_a_device():
         cfg = ob.default_config(**bad)
         assert ob.lib().ouro_create_config(0, 1 << 30, ctypes.byref(cfg), ctypes.byref(out)) == 1, bad
     assert ob.lib().ouro_config_default(None) == 1
+
+
+def test_host_buffer_calls_refuse_bad_arguments_without_a_device():
+    # argument checks come before any CUDA call: a missing heap is refused
+    # (the GPU tests cover the other refusals on a real heap)
+    lib = ob.lib()
+    buf = (ctypes.c_uint64 * 4)()
+    assert lib.ouro_alloc_host(None, 4, 64, None, buf, None, 256, 0, None) == 1
+    assert lib.ouro_free_host(None, 4, buf, 256, 0, None) == 1
+    assert lib.ouro_host_reserve(None, 4) == 1
