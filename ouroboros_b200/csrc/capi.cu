@@ -489,6 +489,16 @@ uint32_t host_slices(uint32_t n, int slices) {
   return k < 1u ? 1u : k > 4u ? 4u : k;
 }
 
+// k slices of m requests (the last one shorter): m = ceil(n / wanted), and
+// k = ceil(n / m), so that every slice starts below n and holds at least one
+// request (n = 10 in 8 wanted slices: 5 slices of 2).
+void host_slice_plan(uint32_t n, int slices, uint32_t* k, uint32_t* m) {
+  const uint64_t want = host_slices(n, slices);
+  const uint64_t per = (n + want - 1u) / want;
+  *m = static_cast<uint32_t>(per);
+  *k = static_cast<uint32_t>((n + per - 1u) / per);
+}
+
 int host_prepare(ouro_heap* h, size_t bytes) {
   if (!h->host_ready) {
     bool ok = cudaStreamCreateWithFlags(&h->host_in, cudaStreamNonBlocking) == cudaSuccess &&
@@ -569,7 +579,8 @@ int ouro_alloc_host(ouro_heap* h, uint32_t n, uint32_t size, const uint32_t* h_s
   uint32_t* d_sizes = h_sizes ? static_cast<uint32_t*>(h->host_stage) : nullptr;
   void** d_ptrs = d_out ? d_out : reinterpret_cast<void**>(static_cast<char*>(h->host_stage) + sizes_bytes);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const uint32_t k = host_slices(n, slices), m = (n + k - 1u) / k;
+  uint32_t k = 0, m = 0;
+  host_slice_plan(n, slices, &k, &m);
   host_enter(h, s);
   rc = dispatch(h->variant, [&](auto v) {
     constexpr int V = decltype(v)::value;
@@ -603,7 +614,8 @@ int ouro_free_host(ouro_heap* h, uint32_t n, void* const* h_ptrs, int block, int
   if (rc) return rc;
   void** d_ptrs = static_cast<void**>(h->host_stage);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const uint32_t k = host_slices(n, slices), m = (n + k - 1u) / k;
+  uint32_t k = 0, m = 0;
+  host_slice_plan(n, slices, &k, &m);
   host_enter(h, s);
   rc = dispatch(h->variant, [&](auto v) {
     constexpr int V = decltype(v)::value;

@@ -95,6 +95,21 @@ def test_back_to_back_calls_share_the_staging():
         _idle(heap)
 
 
+@pytest.mark.parametrize("n,slices", [(1, 8), (10, 8), (7, 3), (33, 0)])
+def test_fewer_requests_than_slices(n, slices):
+    # slices hold ceil(n / slices) requests, and only as many slices as that
+    # takes run (10 requests in 8 wanted slices: 5 slices of 2)
+    with ob.Ouroboros("VAP", GiB) as heap:
+        ptrs = torch.zeros(n, dtype=torch.int64).pin_memory()
+        heap.alloc_host(ptrs, n, 128, slices=slices)
+        torch.cuda.synchronize()
+        _checked(heap, ptrs, n, 128)
+        heap.free_host(ptrs, n, slices=slices)
+        torch.cuda.synchronize()
+        _idle(heap)
+        assert heap.status()["flags"] == 0
+
+
 def test_reserve_then_calls_of_that_size():
     n = 1 << 17
     with ob.Ouroboros("VLC", GiB) as heap:
