@@ -478,26 +478,10 @@ int ouro_free(ouro_heap* h, uint32_t n, void* const* d_ptrs, int block, void* st
 // the work queued on `stream` before the call, and after the previous
 // host-buffer call on this heap (they share the staging), and it ends on
 // `stream`: the caller synchronises `stream` before reading the results.
+using ouro_host::host_slice_plan;
+using ouro_host::kHostSlicesMax;
+
 namespace {
-
-constexpr uint32_t kHostSlicesMax = 8u;
-constexpr uint32_t kHostSliceMin = 1u << 17;   // fewer requests per launch fill the GPU poorly
-
-uint32_t host_slices(uint32_t n, int slices) {
-  if (slices > 0) return n < static_cast<uint32_t>(slices) ? n : static_cast<uint32_t>(slices);
-  const uint32_t k = n / kHostSliceMin;
-  return k < 1u ? 1u : k > 4u ? 4u : k;
-}
-
-// k slices of m requests (the last one shorter): m = ceil(n / wanted), and
-// k = ceil(n / m), so that every slice starts below n and holds at least one
-// request (n = 10 in 8 wanted slices: 5 slices of 2).
-void host_slice_plan(uint32_t n, int slices, uint32_t* k, uint32_t* m) {
-  const uint64_t want = host_slices(n, slices);
-  const uint64_t per = (n + want - 1u) / want;
-  *m = static_cast<uint32_t>(per);
-  *k = static_cast<uint32_t>((n + per - 1u) / per);
-}
 
 int host_prepare(ouro_heap* h, size_t bytes) {
   if (!h->host_ready) {

@@ -8,6 +8,7 @@
 #include <type_traits>
 
 #include "../../include/ouroboros_b200.h"
+#include "host_plan.h"
 #include "ouro/ouroboros.cuh"
 
 struct ouro_heap {
@@ -30,7 +31,7 @@ struct ouro_heap {
   size_t host_stage_bytes;
   cudaStream_t host_in, host_out;
   cudaEvent_t host_entry, host_done, host_joined;
-  cudaEvent_t host_slice_in[8], host_slice_run[8];
+  cudaEvent_t host_slice_in[ouro_host::kHostSlicesMax], host_slice_run[ouro_host::kHostSlicesMax];
   bool host_ready;
   std::mutex host_mu;
 };
